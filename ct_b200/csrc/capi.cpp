@@ -1,0 +1,332 @@
+// extern "C" entry points of libctb (declared in include/ctb.h).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <tuple>
+
+#include "ctb_internal.h"
+#include "host/reconstructor.h"
+
+struct ctb_ctx {
+    ctb::Reconstructor r;
+};
+
+namespace {
+
+// Filter tables cached per (device, W, pad, filter) for the operator layer.
+struct TableKey {
+    int dev, W, pad, filter;
+    bool operator<(const TableKey& o) const {
+        return std::tie(dev, W, pad, filter) < std::tie(o.dev, o.W, o.pad, o.filter);
+    }
+};
+struct Tables {
+    int M = 0, logM = 0;
+    float2* tw = nullptr;
+    float* K = nullptr;
+};
+std::mutex g_tables_mtx;
+std::map<TableKey, Tables> g_tables;
+
+int get_tables(int W, int pad, int filter, cudaStream_t s, Tables* out) {
+    int dev = 0;
+    CTB_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_tables_mtx);
+    const TableKey key{dev, W, pad, filter};
+    auto it = g_tables.find(key);
+    if (it != g_tables.end()) {
+        *out = it->second;
+        return CTB_OK;
+    }
+    Tables t;
+    t.M = ctb::filter_transform_length(W, pad);
+    if (t.M == 0) {
+        ctb::set_global_error("detector width exceeds the largest supported FFT length");
+        return CTB_ERR_UNSUPPORTED;
+    }
+    while ((1 << t.logM) < t.M) ++t.logM;
+    CTB_CUDA_TRY(cudaMalloc(&t.tw, sizeof(float2) * t.M));
+    CTB_CUDA_TRY(cudaMalloc(&t.K, sizeof(float) * t.M));
+    int st = ctb::filter_build_tables(W, pad, filter, t.M, t.tw, t.K, s);
+    if (st != CTB_OK) return st;
+    CTB_CUDA_TRY(cudaStreamSynchronize(s));
+    g_tables[key] = t;
+    *out = t;
+    return CTB_OK;
+}
+
+bool valid_detector(const ctb_detector* d) {
+    return d && d->width > 1 && d->height > 1 && d->fcd > float(d->width) && d->base_intensity != 0.0f;
+}
+
+bool valid_grid(const ctb_grid* g) {
+    return g && g->x_size > 0 && g->y_size > 0 && g->z_size > 0 && g->x_from >= 0 && g->x_to > g->x_from &&
+           g->y_from >= 0 && g->y_to > g->y_from && g->z_from >= 0 && g->z_to > g->z_from && g->voxel_pitch > 0;
+}
+
+int arg_error(const char* msg) {
+    ctb::set_global_error(msg);
+    return CTB_ERR_ARG;
+}
+
+// Device view table {sin, cos, h} from host angle / height arrays.
+int upload_views(const double* ang, const double* h, int n, cudaStream_t s, float4** views) {
+    double* d = nullptr;
+    CTB_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(double) * 2 * n, s));
+    CTB_CUDA_TRY(cudaMallocAsync((void**)views, sizeof(float4) * n, s));
+    CTB_CUDA_TRY(cudaMemcpyAsync(d, ang, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    if (h) {
+        CTB_CUDA_TRY(cudaMemcpyAsync(d + n, h, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    } else {
+        CTB_CUDA_TRY(cudaMemsetAsync(d + n, 0, sizeof(double) * n, s));
+    }
+    int st = ctb::view_table_build(d, d + n, n, *views, s);
+    CTB_CUDA_TRY(cudaFreeAsync(d, s));
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------ operator layer
+int ctb_device_count(int* count) {
+    if (!count) return arg_error("null pointer");
+    return ctb::cuda_status(cudaGetDeviceCount(count), "cudaGetDeviceCount");
+}
+
+int ctb_device_name(int device, char* buf, size_t buf_len) {
+    if (!buf || buf_len == 0) return arg_error("null buffer");
+    cudaDeviceProp p;
+    CTB_CUDA_TRY(cudaGetDeviceProperties(&p, device));
+    std::strncpy(buf, p.name, buf_len - 1);
+    buf[buf_len - 1] = '\0';
+    return CTB_OK;
+}
+
+int ctb_free_memory(int device, size_t* free_bytes, size_t* total_bytes) {
+    int cur = 0;
+    CTB_CUDA_TRY(cudaGetDevice(&cur));
+    CTB_CUDA_TRY(cudaSetDevice(device));
+    size_t f = 0, t = 0;
+    const cudaError_t e = cudaMemGetInfo(&f, &t);
+    cudaSetDevice(cur);
+    CTB_CUDA_TRY(e);
+    if (free_bytes) *free_bytes = f;
+    if (total_bytes) *total_bytes = t;
+    return CTB_OK;
+}
+
+int ctb_reference_grid(ctb_detector* det, const float rel6[6], ctb_grid* grid) {
+    if (!det || !grid || det->width <= 1 || det->height <= 1) return arg_error("invalid detector");
+    float r[6] = {0, 1, 0, 1, 0, 1};
+    if (rel6) {
+        if (rel6[0] == rel6[1] || rel6[2] == rel6[3] || rel6[4] == rel6[5])
+            return arg_error("ERROR: the lower and upper bounds must not be identical.");
+        r[0] = std::max(0.0f, std::min(1.0f, rel6[0]));
+        r[1] = std::max(r[0], std::min(1.0f, rel6[1]));
+        r[2] = std::max(0.0f, std::min(1.0f, rel6[2]));
+        r[3] = std::max(r[0], std::min(1.0f, rel6[3]));
+        r[4] = std::max(0.0f, std::min(1.0f, rel6[4]));
+        r[5] = std::max(r[0], std::min(1.0f, rel6[5]));
+    }
+    const double rad = unsigned(det->width) / 2;
+    const double D = det->fcd;
+    const unsigned radius = unsigned(std::sqrt((D * D * rad * rad) / (D * D + rad * rad)));
+    det->radius = float(radius);
+    grid->x_size = int(2 * radius);
+    grid->y_size = int(2 * radius);
+    grid->z_size = det->height;
+    grid->x_from = int(unsigned(r[0] * grid->x_size + 0.5)); grid->x_to = int(unsigned(r[1] * grid->x_size + 0.5));
+    grid->y_from = int(unsigned(r[2] * grid->y_size + 0.5)); grid->y_to = int(unsigned(r[3] * grid->y_size + 0.5));
+    grid->z_from = int(unsigned(r[4] * grid->z_size + 0.5)); grid->z_to = int(unsigned(r[5] * grid->z_size + 0.5));
+    grid->voxel_pitch = 1.0f;
+    return CTB_OK;
+}
+
+int ctb_filter_projections(const void* raw, int raw_type, int n_views, const ctb_detector* det, int filter,
+                           int pad, void* filtered, int store_type, float store_scale, void* stream) {
+    if (!raw || !filtered || n_views < 0 || !valid_detector(det)) return arg_error("invalid filter arguments");
+    if (raw_type != CTB_U8 && raw_type != CTB_U16 && raw_type != CTB_F32) return arg_error("unknown raw type");
+    if (filter < CTB_RAMLAK || filter > CTB_HANN) return arg_error("unknown filter type");
+    if (pad != 1 && pad != 2) return arg_error("pad must be 1 or 2");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    Tables t;
+    int st = get_tables(det->width, pad, filter, s, &t);
+    if (st != CTB_OK) return st;
+    const ctb::FilterArgs a = ctb::filter_args(*det, raw_type, t.M, t.logM, n_views, store_scale);
+    return ctb::filter_launch(raw, raw_type, filtered, store_type, a, t.tw, t.K, s);
+}
+
+int ctb_backproject(const void* filtered, int store_type, int n_views, const double* angles_deg,
+                    const double* height_offsets_px, const ctb_detector* det, const ctb_grid* grid, int z_begin,
+                    int z_end, float load_scale, float* vol, int accumulate, void* stream) {
+    if (!filtered || !vol || !angles_deg || n_views <= 0 || !valid_detector(det) || !valid_grid(grid))
+        return arg_error("invalid backprojection arguments");
+    if (z_begin < 0 || z_end <= z_begin || z_end > grid->z_to - grid->z_from) return arg_error("invalid z range");
+    if (det->radius <= 0) return arg_error("detector radius not set (use ctb_reference_grid)");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float4* views = nullptr;
+    int st = upload_views(angles_deg, height_offsets_px, n_views, s, &views);
+    if (st != CTB_OK) return st;
+    const ctb::ProjGeom g = ctb::proj_geom(*det, *grid, z_begin, z_end, load_scale);
+    st = ctb::backproject_launch(filtered, store_type, views, n_views, g, vol, accumulate, s);
+    cudaFreeAsync(views, s);
+    return st;
+}
+
+int ctb_forward_project(const float* vol, const double* angles_deg, const double* height_offsets_px, int n_views,
+                        const ctb_detector* det, const ctb_grid* grid, int z_begin, int z_end, float* proj,
+                        int accumulate, void* stream) {
+    if (!vol || !proj || !angles_deg || n_views <= 0 || !valid_detector(det) || !valid_grid(grid))
+        return arg_error("invalid forward projection arguments");
+    if (z_begin < 0 || z_end <= z_begin || z_end > grid->z_to - grid->z_from) return arg_error("invalid z range");
+    if (det->radius <= 0) return arg_error("detector radius not set (use ctb_reference_grid)");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    float4* views = nullptr;
+    int st = upload_views(angles_deg, height_offsets_px, n_views, s, &views);
+    if (st != CTB_OK) return st;
+    const ctb::ProjGeom g = ctb::proj_geom(*det, *grid, z_begin, z_end, 1.0f);
+    st = ctb::forward_launch(vol, views, n_views, g, proj, accumulate, s);
+    cudaFreeAsync(views, s);
+    return st;
+}
+
+int ctb_convert_layout(const float* src, int x, int y, int zs, int index_order, int byte_order, void* dst,
+                       void* stream) {
+    if (!src || !dst) return arg_error("null pointer");
+    return ctb::layout_launch(src, x, y, zs, index_order, byte_order, dst, static_cast<cudaStream_t>(stream));
+}
+
+int ctb_phantom_project(const double* ellipsoids_dev, int n_ellipsoids, const double* angles_deg,
+                        const double* height_offsets_mm, int n_views, int width, int height, double pixel_mm,
+                        double fcd_mm, double u_offset_mm, double* out_dev, void* stream) {
+    if (!ellipsoids_dev || !angles_deg || !out_dev || n_ellipsoids < 0) return arg_error("invalid phantom args");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* d = nullptr;
+    CTB_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(double) * 2 * n_views, s));
+    CTB_CUDA_TRY(cudaMemcpyAsync(d, angles_deg, sizeof(double) * n_views, cudaMemcpyHostToDevice, s));
+    if (height_offsets_mm)
+        CTB_CUDA_TRY(cudaMemcpyAsync(d + n_views, height_offsets_mm, sizeof(double) * n_views, cudaMemcpyHostToDevice, s));
+    else
+        CTB_CUDA_TRY(cudaMemsetAsync(d + n_views, 0, sizeof(double) * n_views, s));
+    int st = ctb::phantom_launch(ellipsoids_dev, n_ellipsoids, d, d + n_views, n_views, width, height, pixel_mm,
+                                 fcd_mm, u_offset_mm, out_dev, s);
+    cudaFreeAsync(d, s);
+    return st;
+}
+
+// ------------------------------------------------------------ facade layer
+int ctb_create(ctb_ctx** ctx) {
+    if (!ctx) return arg_error("null pointer");
+    *ctx = new (std::nothrow) ctb_ctx();
+    return *ctx ? CTB_OK : CTB_ERR_ALLOC;
+}
+
+void ctb_destroy(ctb_ctx* ctx) { delete ctx; }
+
+const char* ctb_last_error(const ctb_ctx* ctx) { return ctx ? ctx->r.error().c_str() : ""; }
+const char* ctb_last_error_global(void) { return ctb::global_error().c_str(); }
+
+#define CTX_CHECK(ctx) \
+    if (!(ctx)) return arg_error("null context")
+
+int ctb_load_csv(ctb_ctx* ctx, const char* csv_path) {
+    CTX_CHECK(ctx);
+    if (!csv_path) return arg_error("null path");
+    return ctx->r.load_csv(csv_path);
+}
+
+int ctb_set_projections(ctb_ctx* ctx, const void* host_images, int raw_type, int n_views, int width, int height,
+                        const double* angles_deg, const double* height_offsets_mm, double pixel_size, int ccw,
+                        double u_offset_mm, double fcd_mm, double base_intensity) {
+    CTX_CHECK(ctx);
+    return ctx->r.set_projections(host_images, raw_type, n_views, width, height, angles_deg, height_offsets_mm,
+                                  pixel_size, ccw, u_offset_mm, fcd_mm, base_intensity);
+}
+
+int ctb_set_volume_bounds(ctb_ctx* ctx, float xmin, float xmax, float ymin, float ymax, float zmin, float zmax) {
+    CTX_CHECK(ctx);
+    return ctx->r.set_bounds(xmin, xmax, ymin, ymax, zmin, zmax);
+}
+int ctb_set_filter(ctb_ctx* ctx, int filter) { CTX_CHECK(ctx); return ctx->r.set_filter(filter); }
+int ctb_set_skip_projections(ctb_ctx* ctx, unsigned skip) { CTX_CHECK(ctx); return ctx->r.set_skip(skip); }
+int ctb_set_device(ctb_ctx* ctx, int device) { CTX_CHECK(ctx); return ctx->r.set_device(device); }
+int ctb_set_gpu_spare_memory(ctb_ctx* ctx, size_t mb) { CTX_CHECK(ctx); return ctx->r.set_spare_mb(mb); }
+int ctb_set_precision(ctb_ctx* ctx, int store_type) { CTX_CHECK(ctx); return ctx->r.set_precision(store_type); }
+int ctb_set_pad(ctb_ctx* ctx, int pad) { CTX_CHECK(ctx); return ctx->r.set_pad(pad); }
+int ctb_set_grid(ctb_ctx* ctx, int x, int y, int z, float vs) { CTX_CHECK(ctx); return ctx->r.set_grid(x, y, z, vs); }
+int ctb_set_slab_height(ctb_ctx* ctx, int slices) { CTX_CHECK(ctx); return ctx->r.set_slab(slices); }
+int ctb_set_progress_callback(ctb_ctx* ctx, ctb_progress_cb cb, void* user) {
+    CTX_CHECK(ctx);
+    ctx->r.set_progress(cb, user);
+    return CTB_OK;
+}
+
+int ctb_get_detector(const ctb_ctx* ctx, ctb_detector* det) {
+    CTX_CHECK(ctx);
+    if (!det) return arg_error("null pointer");
+    *det = ctx->r.detector();
+    return CTB_OK;
+}
+int ctb_get_grid(const ctb_ctx* ctx, ctb_grid* grid) {
+    CTX_CHECK(ctx);
+    if (!grid) return arg_error("null pointer");
+    *grid = ctx->r.grid();
+    return CTB_OK;
+}
+int ctb_get_volume_size(const ctb_ctx* ctx, int* x, int* y, int* z) {
+    CTX_CHECK(ctx);
+    const ctb_grid& g = ctx->r.grid();
+    if (x) *x = g.x_to - g.x_from;
+    if (y) *y = g.y_to - g.y_from;
+    if (z) *z = g.z_to - g.z_from;
+    return CTB_OK;
+}
+int ctb_get_sinogram_size(const ctb_ctx* ctx, int* n) {
+    CTX_CHECK(ctx);
+    if (n) *n = ctx->r.views();
+    return CTB_OK;
+}
+double ctb_get_pixel_size(const ctb_ctx* ctx) { return ctx ? ctx->r.pixel_size() : 0.0; }
+
+int ctb_reconstruct(ctb_ctx* ctx) { CTX_CHECK(ctx); return ctx->r.reconstruct(nullptr, CTB_X_FASTEST); }
+
+int ctb_reconstruct_into(ctb_ctx* ctx, float* host_volume, int index_order) {
+    CTX_CHECK(ctx);
+    if (!host_volume) return arg_error("null output buffer");
+    if (index_order != CTB_X_FASTEST && index_order != CTB_Z_FASTEST) return arg_error("unknown index order");
+    return ctx->r.reconstruct(host_volume, index_order);
+}
+
+int ctb_get_volume(const ctb_ctx* ctx, float* host_volume, int index_order) {
+    CTX_CHECK(ctx);
+    if (!host_volume) return arg_error("null output buffer");
+    return ctx->r.get_volume(host_volume, index_order);
+}
+
+int ctb_save_volume(ctb_ctx* ctx, const char* path, int index_order, int byte_order) {
+    CTX_CHECK(ctx);
+    if (!path) return arg_error("null path");
+    return ctx->r.save(path, index_order, byte_order);
+}
+
+void ctb_stop(ctb_ctx* ctx) {
+    if (ctx) ctx->r.stop();
+}
+
+int ctb_get_timings(const ctb_ctx* ctx, ctb_timings* t) {
+    CTX_CHECK(ctx);
+    if (!t) return arg_error("null pointer");
+    *t = ctx->r.timings();
+    return CTB_OK;
+}
+
+}  // extern "C"

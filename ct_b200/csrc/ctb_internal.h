@@ -1,0 +1,99 @@
+// Internal declarations shared by the kernels (.cu) and the host runtime (.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "../../include/ctb.h"
+
+namespace ctb {
+
+// ----------------------------------------------------------------- errors
+// Thread-local message for context-free calls; contexts keep their own copy.
+void set_global_error(const std::string& msg);
+const std::string& global_error();
+
+// Map a CUDA error to a status, recording the message. Returns CTB_OK on success.
+int cuda_status(cudaError_t e, const char* what);
+
+#define CTB_CUDA_TRY(expr)                                      \
+    do {                                                        \
+        int _st = ::ctb::cuda_status((expr), #expr);            \
+        if (_st != CTB_OK) return _st;                          \
+    } while (0)
+
+inline size_t store_bytes(int store_type) { return store_type == CTB_FP32 ? 4 : 2; }
+inline size_t raw_bytes(int raw_type) { return raw_type == CTB_U8 ? 1 : raw_type == CTB_U16 ? 2 : 4; }
+
+// ----------------------------------------------------------- filter (a)+(b)
+// Largest supported transform: the FFT runs one row pair per group of M/8
+// threads and a CTA has at most 1024 threads.
+constexpr int kMaxFftLen = 8192;
+
+struct FilterPlan {
+    int W = 0, pad = 0, filter = -1, M = 0, logM = 0;
+    float2* tw = nullptr;   // exp(-2 pi i k / M), k < M   (FP64-built, stored FP32)
+    float* K = nullptr;     // real kernel spectrum, M entries (includes scaling)
+};
+
+// Transform length for a detector width and padding mode.
+int filter_transform_length(int W, int pad);
+// Build the twiddle and kernel-spectrum tables on the device (FP64 kernels).
+// tw and K must hold M entries each. Stream-ordered.
+int filter_build_tables(int W, int pad, int filter, int M, float2* tw, float* K, cudaStream_t s);
+
+struct FilterArgs {
+    int W, H, M, logM;
+    long long n_views;
+    float alpha, beta, log_scale;   // convertTo alpha/beta and the log pre-scale
+    float D, uPre, vPre;            // Feldkamp weight
+    float store_scale;
+};
+
+// Launch the fused load/log/weight/FFT/window/IFFT/store kernel over n_views.
+int filter_launch(const void* raw, int raw_type, void* out, int store_type, const FilterArgs& a,
+                  const float2* tw, const float* K, cudaStream_t s);
+
+// Fill FilterArgs from detector geometry (reference preprocessing constants).
+FilterArgs filter_args(const ctb_detector& det, int raw_type, int M, int logM, long long n_views,
+                       float store_scale);
+
+// --------------------------------------------------------- geometry (FP64)
+// Per-view record used by the projector kernels: {sin, cos, heightOffset, 0}.
+// sin/cos follow the reference: float angle_rad = (deg/180)*pi, then the sine
+// of that float in double precision, rounded to float (Ct/CtVolume.cpp:953-955).
+int view_table_build(const double* angles_deg_dev, const double* heights_dev, int n, float4* out,
+                     cudaStream_t s);
+
+// Constants of one backprojection / forward projection launch (slab-local).
+struct ProjGeom {
+    int W, H;
+    int X, Y, Zs;
+    float xPre, yPre, zPre;     // world = (index - pre) * vs ; zPre relative to slab start
+    float vs;
+    float D, uOff, r2;
+    float lbU, ubU, lbV, ubV, uPre, vPre;
+    float load_scale;
+    long long view_stride;      // elements between consecutive projections
+};
+
+ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_end, float load_scale);
+
+// Backprojection of views [0, n) from `views` (device view table) into vol.
+int backproject_launch(const void* proj, int store_type, const float4* views, int n_views,
+                       const ProjGeom& g, float* vol, int accumulate, cudaStream_t s);
+
+int forward_launch(const float* vol, const float4* views, int n_views, const ProjGeom& g, float* proj,
+                   int accumulate, cudaStream_t s);
+
+// ----------------------------------------------------------------- layout
+int layout_launch(const float* src, int x, int y, int zs, int index_order, int byte_order, void* dst,
+                  cudaStream_t s);
+
+// ---------------------------------------------------------------- phantom
+int phantom_launch(const double* ell, int n_ell, const double* angles_deg_dev, const double* heights_mm_dev,
+                   int n_views, int W, int H, double pix, double D, double uoff, double* out, cudaStream_t s);
+
+}  // namespace ctb

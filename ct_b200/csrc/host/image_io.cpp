@@ -1,0 +1,367 @@
+#include "image_io.h"
+
+#include <zlib.h>
+
+#include <algorithm>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <memory>
+
+#include "../../../include/ctb.h"
+
+namespace ctb {
+
+namespace {
+
+bool read_file(const std::string& path, std::vector<uint8_t>* buf, std::string* err) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f.good()) {
+        *err = "cannot open";
+        return false;
+    }
+    f.seekg(0, std::ios::end);
+    const std::streamoff n = f.tellg();
+    if (n <= 0) {
+        *err = "empty file";
+        return false;
+    }
+    f.seekg(0, std::ios::beg);
+    buf->resize(size_t(n));
+    f.read(reinterpret_cast<char*>(buf->data()), n);
+    if (!f) {
+        *err = "read failed";
+        return false;
+    }
+    return true;
+}
+
+size_t sample_bytes(int type) { return type == CTB_U8 ? 1 : type == CTB_U16 ? 2 : 4; }
+
+// ----------------------------------------------------------------- PGM (P5)
+struct PgmHeader {
+    int w = 0, h = 0, maxval = 0;
+    size_t offset = 0;
+};
+
+bool pgm_header(const std::vector<uint8_t>& b, PgmHeader* hd, std::string* err) {
+    if (b.size() < 2 || b[0] != 'P' || b[1] != '5') {
+        *err = "not a binary PGM";
+        return false;
+    }
+    size_t i = 2;
+    int vals[3];
+    for (int k = 0; k < 3; ++k) {
+        while (i < b.size()) {  // skip whitespace and comments
+            if (b[i] == '#') {
+                while (i < b.size() && b[i] != '\n') ++i;
+            } else if (b[i] == ' ' || b[i] == '\t' || b[i] == '\n' || b[i] == '\r') {
+                ++i;
+            } else {
+                break;
+            }
+        }
+        long v = 0;
+        bool any = false;
+        while (i < b.size() && b[i] >= '0' && b[i] <= '9') {
+            v = v * 10 + (b[i] - '0');
+            any = true;
+            ++i;
+            if (v > (1L << 30)) break;
+        }
+        if (!any) {
+            *err = "malformed PGM header";
+            return false;
+        }
+        vals[k] = int(v);
+    }
+    ++i;  // single whitespace before the raster
+    hd->w = vals[0];
+    hd->h = vals[1];
+    hd->maxval = vals[2];
+    hd->offset = i;
+    if (hd->w <= 0 || hd->h <= 0 || hd->maxval <= 0 || hd->maxval > 65535) {
+        *err = "unsupported PGM size or maxval";
+        return false;
+    }
+    return true;
+}
+
+// ----------------------------------------------------------------- TIFF
+struct TiffInfo {
+    int w = 0, h = 0, bps = 0, spp = 1, fmt = 1, comp = 1, photo = 1, planar = 1;
+    long rows_per_strip = -1;
+    std::vector<uint64_t> offsets, counts;
+    bool be = false;
+};
+
+struct Reader {
+    const std::vector<uint8_t>& b;
+    bool be;
+    bool ok = true;
+    uint32_t u16(size_t o) {
+        if (o + 2 > b.size()) { ok = false; return 0; }
+        return be ? (uint32_t(b[o]) << 8) | b[o + 1] : (uint32_t(b[o + 1]) << 8) | b[o];
+    }
+    uint32_t u32(size_t o) {
+        if (o + 4 > b.size()) { ok = false; return 0; }
+        return be ? (uint32_t(b[o]) << 24) | (uint32_t(b[o + 1]) << 16) | (uint32_t(b[o + 2]) << 8) | b[o + 3]
+                  : (uint32_t(b[o + 3]) << 24) | (uint32_t(b[o + 2]) << 16) | (uint32_t(b[o + 1]) << 8) | b[o];
+    }
+};
+
+bool tiff_info(const std::vector<uint8_t>& b, TiffInfo* t, std::string* err) {
+    if (b.size() < 8 || !((b[0] == 'I' && b[1] == 'I') || (b[0] == 'M' && b[1] == 'M'))) {
+        *err = "not a TIFF";
+        return false;
+    }
+    t->be = b[0] == 'M';
+    Reader r{b, t->be};
+    if (r.u16(2) != 42) {
+        *err = "not a classic TIFF";
+        return false;
+    }
+    const size_t ifd = r.u32(4);
+    const uint32_t n = r.u16(ifd);
+    if (!r.ok) {
+        *err = "truncated TIFF";
+        return false;
+    }
+    for (uint32_t k = 0; k < n; ++k) {
+        const size_t e = ifd + 2 + 12 * size_t(k);
+        const uint32_t tag = r.u16(e), typ = r.u16(e + 2), cnt = r.u32(e + 4);
+        auto value = [&](uint32_t idx) -> uint64_t {
+            const size_t sz = typ == 3 ? 2 : 4;
+            const size_t base = (sz * cnt <= 4) ? e + 8 : r.u32(e + 8);
+            return typ == 3 ? r.u16(base + idx * 2) : r.u32(base + idx * 4);
+        };
+        switch (tag) {
+            case 256: t->w = int(value(0)); break;
+            case 257: t->h = int(value(0)); break;
+            case 258: t->bps = int(value(0)); break;
+            case 259: t->comp = int(value(0)); break;
+            case 262: t->photo = int(value(0)); break;
+            case 273: t->offsets.resize(cnt); for (uint32_t i = 0; i < cnt; ++i) t->offsets[i] = value(i); break;
+            case 277: t->spp = int(value(0)); break;
+            case 278: t->rows_per_strip = long(value(0)); break;
+            case 279: t->counts.resize(cnt); for (uint32_t i = 0; i < cnt; ++i) t->counts[i] = value(i); break;
+            case 284: t->planar = int(value(0)); break;
+            case 339: t->fmt = int(value(0)); break;
+            default: break;
+        }
+    }
+    if (!r.ok) {
+        *err = "truncated TIFF directory";
+        return false;
+    }
+    if (t->w <= 0 || t->h <= 0 || t->offsets.empty()) {
+        *err = "TIFF without size or strips";
+        return false;
+    }
+    if (t->comp != 1) {
+        *err = "compressed TIFF is not supported (compression " + std::to_string(t->comp) + ")";
+        return false;
+    }
+    if (t->spp != 1) {
+        *err = "only single-channel TIFF is supported";
+        return false;
+    }
+    return true;
+}
+
+int tiff_type(const TiffInfo& t) {
+    if (t.bps == 8 && t.fmt == 1) return CTB_U8;
+    if (t.bps == 16 && t.fmt == 1) return CTB_U16;
+    if (t.bps == 32 && t.fmt == 3) return CTB_F32;
+    return 0;
+}
+
+// ----------------------------------------------------------------- PNG
+uint32_t be32(const uint8_t* p) { return (uint32_t(p[0]) << 24) | (uint32_t(p[1]) << 16) | (uint32_t(p[2]) << 8) | p[3]; }
+
+struct PngInfo {
+    int w = 0, h = 0, depth = 0, color = 0, interlace = 0;
+    std::vector<uint8_t> idat;
+};
+
+bool png_info(const std::vector<uint8_t>& b, PngInfo* p, bool want_data, std::string* err) {
+    static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
+    if (b.size() < 33 || std::memcmp(b.data(), sig, 8) != 0) {
+        *err = "not a PNG";
+        return false;
+    }
+    size_t i = 8;
+    bool have_ihdr = false;
+    while (i + 12 <= b.size()) {
+        const uint32_t len = be32(&b[i]);
+        const char* type = reinterpret_cast<const char*>(&b[i + 4]);
+        if (i + 12 + size_t(len) > b.size()) {
+            *err = "truncated PNG chunk";
+            return false;
+        }
+        const uint8_t* data = &b[i + 8];
+        if (std::memcmp(type, "IHDR", 4) == 0 && len >= 13) {
+            p->w = int(be32(data));
+            p->h = int(be32(data + 4));
+            p->depth = data[8];
+            p->color = data[9];
+            p->interlace = data[12];
+            have_ihdr = true;
+            if (!want_data) break;
+        } else if (std::memcmp(type, "IDAT", 4) == 0) {
+            p->idat.insert(p->idat.end(), data, data + len);
+        } else if (std::memcmp(type, "IEND", 4) == 0) {
+            break;
+        }
+        i += 12 + size_t(len);
+    }
+    if (!have_ihdr) {
+        *err = "PNG without IHDR";
+        return false;
+    }
+    if (p->color != 0) {
+        *err = "only grayscale PNG is supported";
+        return false;
+    }
+    if (p->interlace != 0) {
+        *err = "interlaced PNG is not supported";
+        return false;
+    }
+    if (p->depth != 8 && p->depth != 16) {
+        *err = "only 8/16-bit PNG is supported";
+        return false;
+    }
+    return true;
+}
+
+bool png_decode(PngInfo& p, void* dst, std::string* err) {
+    const size_t bpp = p.depth / 8;
+    const size_t stride = size_t(p.w) * bpp;
+    std::vector<uint8_t> raw((stride + 1) * size_t(p.h));
+    uLongf out_len = uLongf(raw.size());
+    if (uncompress(raw.data(), &out_len, p.idat.data(), uLong(p.idat.size())) != Z_OK || out_len != raw.size()) {
+        *err = "PNG inflate failed";
+        return false;
+    }
+    std::vector<uint8_t> prev(stride, 0), cur(stride);
+    uint8_t* out = static_cast<uint8_t*>(dst);
+    for (int r = 0; r < p.h; ++r) {
+        const uint8_t f = raw[size_t(r) * (stride + 1)];
+        const uint8_t* src = &raw[size_t(r) * (stride + 1) + 1];
+        for (size_t c = 0; c < stride; ++c) {
+            const int a = c >= bpp ? cur[c - bpp] : 0, up = prev[c], ul = c >= bpp ? prev[c - bpp] : 0;
+            int v = src[c];
+            switch (f) {
+                case 0: break;
+                case 1: v += a; break;
+                case 2: v += up; break;
+                case 3: v += (a + up) / 2; break;
+                case 4: {
+                    const int pp = a + up - ul, pa = std::abs(pp - a), pb = std::abs(pp - up), pc = std::abs(pp - ul);
+                    v += (pa <= pb && pa <= pc) ? a : (pb <= pc ? up : ul);
+                    break;
+                }
+                default: *err = "bad PNG filter"; return false;
+            }
+            cur[c] = uint8_t(v);
+        }
+        if (bpp == 1) {
+            std::memcpy(out + size_t(r) * stride, cur.data(), stride);
+        } else {
+            uint16_t* o = reinterpret_cast<uint16_t*>(out) + size_t(r) * p.w;
+            for (int c = 0; c < p.w; ++c) o[c] = uint16_t((cur[2 * c] << 8) | cur[2 * c + 1]);
+        }
+        std::swap(prev, cur);
+    }
+    return true;
+}
+
+}  // namespace
+
+bool probe_image(const std::string& path, int* width, int* height, int* type, std::string* err) {
+    std::vector<uint8_t> b;
+    if (!read_file(path, &b, err)) return false;
+    if (b.size() >= 2 && b[0] == 'P' && b[1] == '5') {
+        PgmHeader hd;
+        if (!pgm_header(b, &hd, err)) return false;
+        *width = hd.w; *height = hd.h; *type = hd.maxval < 256 ? CTB_U8 : CTB_U16;
+        return true;
+    }
+    if (b.size() >= 4 && (b[0] == 'I' || b[0] == 'M')) {
+        TiffInfo t;
+        if (!tiff_info(b, &t, err)) return false;
+        *width = t.w; *height = t.h; *type = tiff_type(t);
+        if (!*type) { *err = "unsupported TIFF sample format"; return false; }
+        return true;
+    }
+    if (b.size() >= 8 && b[0] == 137 && b[1] == 'P') {
+        PngInfo p;
+        if (!png_info(b, &p, false, err)) return false;
+        *width = p.w; *height = p.h; *type = p.depth == 8 ? CTB_U8 : CTB_U16;
+        return true;
+    }
+    *err = "unsupported image format";
+    return false;
+}
+
+bool decode_image_into(const std::string& path, int width, int height, int type, void* dst, std::string* err) {
+    std::vector<uint8_t> b;
+    if (!read_file(path, &b, err)) return false;
+    const size_t n = size_t(width) * height;
+    if (b.size() >= 2 && b[0] == 'P' && b[1] == '5') {
+        PgmHeader hd;
+        if (!pgm_header(b, &hd, err)) return false;
+        const int t = hd.maxval < 256 ? CTB_U8 : CTB_U16;
+        if (hd.w != width || hd.h != height || t != type) { *err = "size or depth differs"; return false; }
+        if (b.size() < hd.offset + n * sample_bytes(t)) { *err = "truncated PGM raster"; return false; }
+        const uint8_t* src = b.data() + hd.offset;
+        if (t == CTB_U8) {
+            std::memcpy(dst, src, n);
+        } else {
+            uint16_t* o = static_cast<uint16_t*>(dst);
+            for (size_t i = 0; i < n; ++i) o[i] = uint16_t((src[2 * i] << 8) | src[2 * i + 1]);
+        }
+        return true;
+    }
+    if (b.size() >= 4 && (b[0] == 'I' || b[0] == 'M')) {
+        TiffInfo t;
+        if (!tiff_info(b, &t, err)) return false;
+        const int ty = tiff_type(t);
+        if (t.w != width || t.h != height || ty != type) { *err = "size or depth differs"; return false; }
+        const size_t sb = sample_bytes(ty), row = size_t(width) * sb;
+        const long rps = t.rows_per_strip > 0 ? t.rows_per_strip : height;
+        uint8_t* o = static_cast<uint8_t*>(dst);
+        size_t written = 0;
+        for (size_t s = 0; s < t.offsets.size() && written < n * sb; ++s) {
+            const size_t rows = std::min<size_t>(size_t(rps), size_t(height) - s * size_t(rps));
+            const size_t bytes = rows * row;
+            if (t.offsets[s] + bytes > b.size()) { *err = "truncated TIFF strip"; return false; }
+            std::memcpy(o + written, b.data() + t.offsets[s], bytes);
+            written += bytes;
+        }
+        if (written != n * sb) { *err = "TIFF strips do not cover the image"; return false; }
+        if (t.be && sb > 1) {
+            for (size_t i = 0; i < n; ++i) std::reverse(o + i * sb, o + (i + 1) * sb);
+        }
+        return true;
+    }
+    if (b.size() >= 8 && b[0] == 137 && b[1] == 'P') {
+        PngInfo p;
+        if (!png_info(b, &p, true, err)) return false;
+        const int t = p.depth == 8 ? CTB_U8 : CTB_U16;
+        if (p.w != width || p.h != height || t != type) { *err = "size or depth differs"; return false; }
+        return png_decode(p, dst, err);
+    }
+    *err = "unsupported image format";
+    return false;
+}
+
+bool decode_image(const std::string& path, Image* img, std::string* err) {
+    if (!probe_image(path, &img->width, &img->height, &img->type, err)) return false;
+    img->data.resize(size_t(img->width) * img->height * sample_bytes(img->type));
+    return decode_image_into(path, img->width, img->height, img->type, img->data.data(), err);
+}
+
+}  // namespace ctb

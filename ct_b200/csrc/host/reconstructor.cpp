@@ -1,0 +1,689 @@
+// Reconstruction facade implementation (ct::CtVolume counterpart).
+//
+// Pipeline of one reconstruction on one B200 (all views' filtered projections
+// stay resident in HBM; the volume streams out in z-slabs):
+//   copy stream    : H2D of raw u8/u16/f32 projections in chunks of views,
+//                    into a 3-slot ring of device buffers
+//   compute stream : fused preprocess + ramp filter of each chunk (kernel a+b)
+//                    into the resident filtered set (FP32/FP16/BF16), then
+//                    one backprojection launch per z-slab over all views
+//                    (kernel c), then the output layout kernel
+//   download stream: D2H of each finished slab while the next slab computes
+// The reference instead re-reads and re-filters every projection for every
+// VRAM-sized chunk and launches one kernel per view (Ct/CtVolume.cpp:1155-1301).
+
+#include "reconstructor.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <thread>
+
+#include "image_io.h"
+
+namespace ctb {
+
+// ------------------------------------------------------------------ buffers
+int DevBuf::ensure(size_t n, const char* what) {
+    if (n <= bytes && p) return CTB_OK;
+    release();
+    if (n == 0) return CTB_OK;
+    cudaError_t e = cudaMalloc(&p, n);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cudaGetLastError();
+        set_global_error(std::string("device allocation of ") + std::to_string(n >> 20) + " MB for " + what +
+                         " failed: " + cudaGetErrorString(e));
+        return CTB_ERR_ALLOC;
+    }
+    bytes = n;
+    return CTB_OK;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+}
+
+int HostBuf::ensure(size_t n) {
+    if (n <= bytes && p) return CTB_OK;
+    release();
+    if (n == 0) return CTB_OK;
+    if (cudaHostAlloc(&p, n, cudaHostAllocPortable) == cudaSuccess) {
+        pinned = true;
+    } else {
+        cudaGetLastError();
+        p = std::malloc(n);
+        pinned = false;
+        if (!p) return CTB_ERR_ALLOC;
+    }
+    bytes = n;
+    return CTB_OK;
+}
+void HostBuf::release() {
+    if (p) {
+        if (pinned) cudaFreeHost(p);
+        else std::free(p);
+    }
+    p = nullptr;
+    bytes = 0;
+    pinned = false;
+}
+
+namespace {
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Multi-threaded host loop over [0, n).
+template <typename F>
+void parallel_for(size_t n, F&& f) {
+    const size_t T = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (n < 2 * T) {
+        for (size_t i = 0; i < n; ++i) f(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (size_t t = 0; t < T; ++t)
+        th.emplace_back([&, t] {
+            for (size_t i = t * n / T; i < (t + 1) * n / T; ++i) f(i);
+        });
+    for (auto& x : th) x.join();
+}
+
+// QString::toDouble semantics: the whole field must be a number (surrounding
+// whitespace allowed).
+bool to_double(const std::string& s, double* out) {
+    const char* b = s.c_str();
+    char* e = nullptr;
+    *out = std::strtod(b, &e);
+    if (e == b) return false;
+    while (*e == ' ' || *e == '\t' || *e == '\r' || *e == '\n') ++e;
+    return *e == '\0';
+}
+
+std::string first_field(const std::string& line) { return line.substr(0, line.find('\t')); }
+
+std::vector<std::string> split_tabs(const std::string& line) {
+    std::vector<std::string> f;
+    size_t a = 0;
+    while (true) {
+        size_t b = line.find('\t', a);
+        f.push_back(line.substr(a, b == std::string::npos ? std::string::npos : b - a));
+        if (b == std::string::npos) break;
+        a = b + 1;
+    }
+    return f;
+}
+
+std::string dirname_of(const std::string& p) {
+    size_t k = p.find_last_of('/');
+    return k == std::string::npos ? std::string(".") : p.substr(0, k);
+}
+
+std::string join_path(const std::string& dir, const std::string& name) {
+    if (!name.empty() && name[0] == '/') return name;
+    if (dir.empty()) return name;
+    return dir.back() == '/' ? dir + name : dir + "/" + name;
+}
+
+unsigned cylinder_radius(int W, float FCD) {
+    // getReconstructionCylinderRadius (Ct/CtVolume.cpp:370-373)
+    double radius = unsigned(W) / 2;
+    return unsigned(std::sqrt((double(FCD) * FCD * radius * radius) / (double(FCD) * FCD + radius * radius)));
+}
+
+}  // namespace
+
+Reconstructor::Reconstructor() {}
+
+Reconstructor::~Reconstructor() {
+    if (s_copy_) {
+        cudaSetDevice(device_);
+        cudaStreamDestroy(s_copy_);
+        cudaStreamDestroy(s_comp_);
+        cudaStreamDestroy(s_down_);
+    }
+}
+
+int Reconstructor::fail(int status, const std::string& msg) {
+    err_ = msg;
+    set_global_error(msg);
+    return status;
+}
+
+// updateBoundaries (Ct/CtVolume.cpp:1399-1424) on the reference grid rule
+// (:311-316) or on the overriding grid.
+void Reconstructor::update_grid() {
+    const unsigned radius = cylinder_radius(det_.width, det_.fcd);
+    det_.radius = float(radius);
+    ctb_grid g{};
+    if (grid_x_ > 0) {
+        g.x_size = grid_x_; g.y_size = grid_y_; g.z_size = grid_z_;
+        g.voxel_pitch = grid_vs_;
+    } else {
+        g.x_size = int(radius * 2); g.y_size = int(radius * 2); g.z_size = det_.height;
+        g.voxel_pitch = 1.0f;
+    }
+    g.x_from = int(unsigned(rel_[0] * g.x_size + 0.5)); g.x_to = int(unsigned(rel_[1] * g.x_size + 0.5));
+    g.y_from = int(unsigned(rel_[2] * g.y_size + 0.5)); g.y_to = int(unsigned(rel_[3] * g.y_size + 0.5));
+    g.z_from = int(unsigned(rel_[4] * g.z_size + 0.5)); g.z_to = int(unsigned(rel_[5] * g.z_size + 0.5));
+    grid_ = g;
+}
+
+// setVolumeBounds (Ct/CtVolume.cpp:487-500), including the reference's clamp
+// of the y/z upper bounds against xFrom.
+int Reconstructor::set_bounds(float xF, float xT, float yF, float yT, float zF, float zT) {
+    std::lock_guard<std::mutex> lk(mtx_);
+    if (xF == xT || yF == yT || zF == zT)
+        return fail(CTB_ERR_ARG, "ERROR: the lower and upper bounds must not be identical.");
+    rel_[0] = std::max(0.0f, std::min(1.0f, xF));
+    rel_[1] = std::max(rel_[0], std::min(1.0f, xT));
+    rel_[2] = std::max(0.0f, std::min(1.0f, yF));
+    rel_[3] = std::max(rel_[0], std::min(1.0f, yT));
+    rel_[4] = std::max(0.0f, std::min(1.0f, zF));
+    rel_[5] = std::max(rel_[0], std::min(1.0f, zT));
+    if (have_scan_) update_grid();
+    return CTB_OK;
+}
+
+int Reconstructor::set_filter(int f) {
+    if (f < CTB_RAMLAK || f > CTB_HANN) return fail(CTB_ERR_ARG, "unknown filter type");
+    filter_ = f;
+    return CTB_OK;
+}
+
+int Reconstructor::set_device(int d) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || d < 0 || d >= n) {
+        cudaGetLastError();
+        return fail(CTB_ERR_ARG, "Active CUDA device was not set because the device ID is not valid.");
+    }
+    if (s_copy_ && d != device_) {
+        cudaSetDevice(device_);
+        cudaStreamDestroy(s_copy_); cudaStreamDestroy(s_comp_); cudaStreamDestroy(s_down_);
+        s_copy_ = s_comp_ = s_down_ = nullptr;
+        d_filtered_.release(); d_ring_.release(); d_views_.release(); d_angles_.release();
+        d_heights_.release(); d_tw_.release(); d_K_.release();
+        for (auto& b : d_slab_) b.release();
+        for (auto& b : d_conv_) b.release();
+        tables_key_[0] = -1;
+    }
+    device_ = d;
+    return CTB_OK;
+}
+
+int Reconstructor::set_precision(int t) {
+    if (t != CTB_FP32 && t != CTB_FP16 && t != CTB_BF16) return fail(CTB_ERR_ARG, "unknown storage type");
+    store_ = t;
+    return CTB_OK;
+}
+
+int Reconstructor::set_pad(int p) {
+    if (p != 1 && p != 2) return fail(CTB_ERR_ARG, "pad must be 1 or 2");
+    pad_ = p;
+    return CTB_OK;
+}
+
+int Reconstructor::set_grid(int x, int y, int z, float vs) {
+    if (x == 0 && y == 0 && z == 0) {
+        grid_x_ = grid_y_ = grid_z_ = 0;
+        grid_vs_ = 1.0f;
+    } else {
+        if (x <= 0 || y <= 0 || z <= 0 || !(vs > 0)) return fail(CTB_ERR_ARG, "invalid grid");
+        grid_x_ = x; grid_y_ = y; grid_z_ = z; grid_vs_ = vs;
+    }
+    if (have_scan_) update_grid();
+    return CTB_OK;
+}
+
+// sinogramFromImages (Ct/CtVolume.cpp:136-330).
+int Reconstructor::load_csv(const std::string& csv_path) {
+    std::lock_guard<std::mutex> lk(mtx_);
+    stop_ = false;
+    have_scan_ = false;
+    angles_.clear();
+    heights_px_.clear();
+    std::ifstream in(csv_path);
+    if (!in.good()) return fail(CTB_ERR_IO, "Could not open the config file.");
+    std::vector<std::string> lines;
+    {
+        std::string l;
+        while (std::getline(in, l)) {
+            if (!l.empty() && l.back() == '\r') l.pop_back();
+            lines.push_back(l);
+        }
+    }
+    auto line_at = [&](size_t i) { return i < lines.size() ? lines[i] : std::string(); };
+    // header :157-168
+    std::string image_dir = first_field(line_at(0));
+    double pix = 0, uoff = 0, fcd = 0, base = 0;
+    bool ok = to_double(first_field(line_at(1)), &pix);
+    const std::string rotation = first_field(line_at(2));
+    ok = to_double(first_field(line_at(3)), &uoff) && ok;
+    ok = to_double(first_field(line_at(4)), &fcd) && ok;
+    ok = to_double(first_field(line_at(5)), &base) && ok;
+    if (!ok) return fail(CTB_ERR_CSV, "Could not read the parameters from the CSV file successfully.");
+    if (float(base) == 0.0f)
+        return fail(CTB_ERR_CSV,
+                    "Error: The base intensity given in the configuration file must not be equal to zero.");
+    // relative image directory is resolved against the CSV's directory (:185-187)
+    if (image_dir.empty() || image_dir[0] != '/') image_dir = join_path(dirname_of(csv_path), image_dir);
+
+    // image lines :197-213 (a line with fewer than two fields repeats the
+    // previous file name and angle, as in the reference)
+    std::vector<std::string> paths;
+    std::vector<double> ang, hmm;
+    std::string fname;
+    double a = 0, h = 0;
+    bool all_ok = true;
+    for (size_t i = 7; i < lines.size(); ++i) {
+        const std::vector<std::string> f = split_tabs(lines[i]);
+        if (f.size() >= 2) {
+            fname = f[0];
+            double v;
+            const bool s = to_double(f[1], &v);
+            all_ok = all_ok && s;
+            a = v;
+        }
+        if (f.size() >= 3) {
+            double v;
+            const bool s = to_double(f[2], &v);
+            all_ok = all_ok && s;
+            h = v;
+        } else {
+            h = 0;
+        }
+        paths.push_back(join_path(image_dir, fname));
+        ang.push_back(a);
+        hmm.push_back(h);
+    }
+    if (!all_ok) return fail(CTB_ERR_CSV, "Could not read the image parameters from the CSV file successfully.");
+    if (paths.empty()) return fail(CTB_ERR_CSV, "Apparently the config file does not contain any images.");
+
+    // probe the first image, then decode all into pinned host memory (:227-292)
+    int W = 0, H = 0, type = 0;
+    std::string e;
+    if (!probe_image(paths[0], &W, &H, &type, &e))
+        return fail(CTB_ERR_IMAGE, "Error loading the image \"" + paths[0] +
+                                       "\". Maybe it does not exist, permissions are missing or the format is "
+                                       "not supported. (" + e + ")");
+    const size_t bytes_per = size_t(W) * H * raw_bytes(type);
+    if (images_owned_.ensure(bytes_per * paths.size()) != CTB_OK)
+        return fail(CTB_ERR_ALLOC, "Host memory for the projections could not be allocated.");
+    std::atomic<int> bad{-1};
+    std::vector<std::string> errs(paths.size());
+    std::atomic<size_t> done{0};
+    parallel_for(paths.size(), [&](size_t i) {
+        if (bad.load() >= 0 || stop_) return;
+        int w = 0, hh = 0, t = 0;
+        std::string er;
+        bool good = probe_image(paths[i], &w, &hh, &t, &er);
+        if (good && (w != W || hh != H)) { good = false; er = "dims"; }
+        if (good && t != type) { good = false; er = "depth"; }
+        if (good) good = decode_image_into(paths[i], W, H, type, (char*)images_owned_.p + i * bytes_per, &er);
+        if (!good) {
+            errs[i] = er;
+            int expect = -1;
+            bad.compare_exchange_strong(expect, int(i));
+        }
+        done++;
+    });
+    if (stop_) return fail(CTB_INTERRUPTED, "User interrupted. Stopping.");
+    if (bad.load() >= 0) {
+        const size_t i = size_t(bad.load());
+        if (errs[i] == "dims")
+            return fail(CTB_ERR_IMAGE, "Error loading the image \"" + paths[i] +
+                                           "\", its dimensions differ from the images before.");
+        if (errs[i] == "depth")
+            return fail(CTB_ERR_IMAGE, "Error loading the image \"" + paths[i] +
+                                           "\". All images must have the same depth (8bit, 16bit or 32bit).");
+        return fail(CTB_ERR_IMAGE, "Error loading the image \"" + paths[i] +
+                                       "\". Maybe it does not exist, permissions are missing or the format is "
+                                       "not supported. (" + errs[i] + ")");
+    }
+    progress(0, 100.0);
+    images_ = images_owned_.p;
+    return assign_scan(images_owned_.p, type, int(paths.size()), W, H, ang.data(), hmm.data(), pix,
+                       rotation == "ccw" ? 1 : (rotation == "cw" ? 0 : -1), uoff, fcd, base);
+}
+
+int Reconstructor::set_projections(const void* images, int raw_type, int n_views, int width, int height,
+                                   const double* angles_deg, const double* heights_mm, double pixel_size,
+                                   int ccw, double u_offset_mm, double fcd_mm, double base_intensity) {
+    std::lock_guard<std::mutex> lk(mtx_);
+    stop_ = false;
+    have_scan_ = false;
+    return assign_scan(images, raw_type, n_views, width, height, angles_deg, heights_mm, pixel_size, ccw,
+                       u_offset_mm, fcd_mm, base_intensity);
+}
+
+// Shared tail of the CSV path and the in-memory entry point: FCD/uOffset in
+// pixels (:170-172), the W >= FCD check (:294-301), relative height offsets
+// (:742-753), direction correction (:755-767) and the grid (:311-316).
+// ccw: 1 = "ccw", 0 = "cw", -1 = any other string (no correction).
+int Reconstructor::assign_scan(const void* images, int raw_type, int n_views, int width, int height,
+                               const double* angles_deg, const double* heights_mm, double pixel_size, int ccw,
+                               double u_offset_mm, double fcd_mm, double base_intensity) {
+    if (!images || n_views <= 0 || width <= 1 || height <= 1 || !angles_deg)
+        return fail(CTB_ERR_ARG, "invalid projection set");
+    if (raw_type != CTB_U8 && raw_type != CTB_U16 && raw_type != CTB_F32)
+        return fail(CTB_ERR_IMAGE, "The image depth must be either 8bit, 16bit or 32bit.");
+    if (float(base_intensity) == 0.0f)
+        return fail(CTB_ERR_CSV,
+                    "Error: The base intensity given in the configuration file must not be equal to zero.");
+    const float pix = float(pixel_size);
+    float FCD = float(fcd_mm);
+    FCD /= pix;
+    float uOffset = float(u_offset_mm);
+    uOffset /= pix;
+    if (float(width) >= FCD) {
+        have_scan_ = false;
+        return fail(CTB_ERR_ARG, "Error: the FCD must be greater than the image width.");
+    }
+    det_.width = width;
+    det_.height = height;
+    det_.fcd = FCD;
+    det_.u_offset = uOffset;
+    det_.base_intensity = float(base_intensity);
+    pixel_size_ = pix;
+    raw_type_ = raw_type;
+    images_ = images;
+    angles_.assign(angles_deg, angles_deg + n_views);
+    heights_px_.assign(n_views, 0.0);
+    if (heights_mm) heights_px_.assign(heights_mm, heights_mm + n_views);
+    double sum = 0;
+    for (double v : heights_px_) sum += v;
+    sum /= double(n_views);
+    for (double& v : heights_px_) { v -= sum; v /= double(pix); }
+    if (n_views > 1 && ccw >= 0) {
+        const double diff = angles_[1] - angles_[0];
+        if ((ccw == 0 && diff > 0) || (ccw == 1 && diff < 0))
+            for (double& v : angles_) v *= -1;
+    }
+    have_scan_ = true;
+    update_grid();
+    return CTB_OK;
+}
+
+int Reconstructor::reconstruct(float* host_out, int index_order) {
+    std::lock_guard<std::mutex> lk(mtx_);
+    stop_ = false;
+    if (!have_scan_)
+        return fail(CTB_ERR_ARG, "Volume was not reconstructed, because the sinogram seems to be empty. Please "
+                                 "load some images first.");
+    const int X = grid_.x_to - grid_.x_from, Y = grid_.y_to - grid_.y_from, Z = grid_.z_to - grid_.z_from;
+    if (X <= 0 || Y <= 0 || Z <= 0) return fail(CTB_ERR_ARG, "The reconstructed box is empty.");
+    float* target = host_out;
+    if (!target) {
+        if (volume_.ensure(sizeof(float) * size_t(X) * Y * Z) != CTB_OK)
+            return fail(CTB_ERR_ALLOC,
+                        "The memory allocation for the volume failed. Maybe there is not enought free RAM.");
+        target = static_cast<float*>(volume_.p);
+        index_order = CTB_X_FASTEST;
+    }
+    const int st = run_pipeline(target, index_order);
+    if (st != CTB_OK) {
+        if (!host_out) vol_dims_[0] = vol_dims_[1] = vol_dims_[2] = 0;  // volume.clear() (:617)
+        return st;
+    }
+    if (!host_out) { vol_dims_[0] = X; vol_dims_[1] = Y; vol_dims_[2] = Z; }
+    return CTB_OK;
+}
+
+int Reconstructor::run_pipeline(float* out, int order) {
+    const auto t_start = std::chrono::steady_clock::now();
+    if (cudaSetDevice(device_) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(CTB_ERR_CUDA, "CUDA device could not be selected.");
+    }
+    if (!s_copy_) {
+        if (cudaStreamCreateWithFlags(&s_copy_, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&s_comp_, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&s_down_, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CTB_ERR_CUDA, "CUDA streams could not be created.");
+        }
+    }
+    const int W = det_.width, H = det_.height;
+    const int X = grid_.x_to - grid_.x_from, Y = grid_.y_to - grid_.y_from, Z = grid_.z_to - grid_.z_from;
+
+    // views used (setSkipProjections: projectionStep, :945)
+    std::vector<int> used;
+    for (int p = 0; p < int(angles_.size()); p += std::max(1, step_)) used.push_back(p);
+    const int V = int(used.size());
+    std::vector<double> ang(V), hp(V);
+    for (int i = 0; i < V; ++i) { ang[i] = angles_[used[i]]; hp[i] = heights_px_[used[i]]; }
+
+    const int M = filter_transform_length(W, pad_);
+    if (M == 0) return fail(CTB_ERR_UNSUPPORTED, "Detector width exceeds the largest supported FFT length.");
+    int logM = 0;
+    while ((1 << logM) < M) ++logM;
+
+    // storage scale: FP16/BF16 keep values near unit magnitude (x 1/W)
+    const float store_scale = store_ == CTB_FP32 ? 1.0f : 1.0f / float(W);
+    const float load_scale = store_ == CTB_FP32 ? 1.0f : float(W);
+
+    // ---- sizing
+    const size_t view_raw = size_t(W) * H * raw_bytes(raw_type_);
+    const size_t view_filt = size_t(W) * H * store_bytes(store_);
+    const int chunk = int(std::max<size_t>(1, std::min<size_t>(size_t(V), (size_t(256) << 20) / view_raw)));
+    const size_t plane = size_t(X) * Y;
+    int slab = slab_req_ > 0 ? slab_req_ : std::max(16, ((Z + 7) / 8 + 15) / 16 * 16);
+    slab = std::min(slab, Z);
+    const bool convert = order == CTB_Z_FASTEST;
+    {
+        size_t freeb = 0, total = 0;
+        cudaMemGetInfo(&freeb, &total);
+        const size_t spare = spare_mb_ << 20;
+        auto need = [&](int sl) {
+            return view_filt * V + 3 * view_raw * chunk + 2 * plane * sl * 4 * (convert ? 2 : 1) + 64 * V +
+                   size_t(M) * 12;
+        };
+        const size_t have = d_filtered_.bytes + d_ring_.bytes + d_slab_[0].bytes * 2 + d_conv_[0].bytes * 2;
+        while (slab > 16 && need(slab) > freeb + have - std::min(freeb + have, spare)) slab = std::max(16, slab / 2);
+        if (need(slab) + spare > freeb + have)
+            return fail(CTB_ERR_ALLOC,
+                        "An error occured during allocation of memory for the volume in the VRAM. Maybe the amount "
+                        "of free VRAM was insufficient. You can try changing the GPU spare memory setting.");
+    }
+    int st;
+    if ((st = d_filtered_.ensure(view_filt * V, "filtered projections")) ||
+        (st = d_ring_.ensure(3 * view_raw * chunk, "projection upload ring")) ||
+        (st = d_views_.ensure(sizeof(float4) * V, "view table")) ||
+        (st = d_angles_.ensure(sizeof(double) * V, "angles")) ||
+        (st = d_heights_.ensure(sizeof(double) * V, "height offsets")) ||
+        (st = d_tw_.ensure(sizeof(float2) * M, "twiddles")) || (st = d_K_.ensure(sizeof(float) * M, "filter")))
+        return fail(st, global_error());
+    for (int b = 0; b < 2; ++b) {
+        if ((st = d_slab_[b].ensure(sizeof(float) * plane * slab, "volume slab"))) return fail(st, global_error());
+        if (convert && (st = d_conv_[b].ensure(sizeof(float) * plane * slab, "layout slab")))
+            return fail(st, global_error());
+    }
+    const bool out_pinned = is_pinned(out);
+    if (!out_pinned)
+        for (auto& hb : h_stage_)
+            if (hb.ensure(sizeof(float) * plane * slab) != CTB_OK || !hb.pinned)
+                return fail(CTB_ERR_ALLOC, "Pinned staging memory could not be allocated.");
+
+    // ---- events
+    cudaEvent_t ev_up[3], ev_free[3], ev_bp[2], ev_down[2], e_f0, e_f1, e_b0, e_b1;
+    const int nchunks = (V + chunk - 1) / chunk;
+    const int nslabs = (Z + slab - 1) / slab;
+    std::vector<cudaEvent_t> tf(2 * nchunks), tb(2 * nslabs);
+    for (auto& e : tf) cudaEventCreate(&e);
+    for (auto& e : tb) cudaEventCreate(&e);
+    for (auto& e : ev_up) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    for (auto& e : ev_free) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    for (auto& e : ev_bp) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    for (auto& e : ev_down) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    cudaEventCreate(&e_f0); cudaEventCreate(&e_f1); cudaEventCreate(&e_b0); cudaEventCreate(&e_b1);
+    auto cleanup = [&]() {
+        for (auto& e : ev_up) cudaEventDestroy(e);
+        for (auto& e : ev_free) cudaEventDestroy(e);
+        for (auto& e : ev_bp) cudaEventDestroy(e);
+        for (auto& e : ev_down) cudaEventDestroy(e);
+        cudaEventDestroy(e_f0); cudaEventDestroy(e_f1); cudaEventDestroy(e_b0); cudaEventDestroy(e_b1);
+        for (auto& e : tf) cudaEventDestroy(e);
+        for (auto& e : tb) cudaEventDestroy(e);
+    };
+    auto cuda_fail = [&](const char* what) {
+        cudaStreamSynchronize(s_copy_); cudaStreamSynchronize(s_comp_); cudaStreamSynchronize(s_down_);
+        cleanup();
+        const cudaError_t e = cudaGetLastError();
+        return fail(CTB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+
+    // ---- geometry tables (FP64 kernels)
+    if (cudaMemcpyAsync(d_angles_.p, ang.data(), sizeof(double) * V, cudaMemcpyHostToDevice, s_comp_) ||
+        cudaMemcpyAsync(d_heights_.p, hp.data(), sizeof(double) * V, cudaMemcpyHostToDevice, s_comp_))
+        return cuda_fail("geometry upload");
+    if (view_table_build((double*)d_angles_.p, (double*)d_heights_.p, V, (float4*)d_views_.p, s_comp_))
+        return cuda_fail("view table");
+    if (tables_key_[0] != W || tables_key_[1] != pad_ || tables_key_[2] != filter_) {
+        if (filter_build_tables(W, pad_, filter_, M, (float2*)d_tw_.p, (float*)d_K_.p, s_comp_))
+            return cuda_fail("filter tables");
+        tables_key_[0] = W; tables_key_[1] = pad_; tables_key_[2] = filter_;
+    }
+    // the ring slots start free
+    for (auto& e : ev_free) cudaEventRecord(e, s_comp_);
+
+    // ---- upload + filter
+    const bool in_pinned = is_pinned(images_);
+    cudaEventRecord(e_f0, s_comp_);
+    int slot = 0;
+    for (int c0 = 0; c0 < V; c0 += chunk, slot = (slot + 1) % 3) {
+        if (stop_) { cuda_fail("stop"); return fail(CTB_INTERRUPTED, "User interrupted. Stopping."); }
+        const int n = std::min(chunk, V - c0);
+        char* dst = (char*)d_ring_.p + size_t(slot) * view_raw * chunk;
+        cudaStreamWaitEvent(s_copy_, ev_free[slot], 0);
+        if (step_ <= 1) {
+            if (cudaMemcpyAsync(dst, (const char*)images_ + size_t(c0) * view_raw, view_raw * n,
+                                cudaMemcpyHostToDevice, s_copy_))
+                return cuda_fail("projection upload");
+        } else {
+            for (int i = 0; i < n; ++i)
+                if (cudaMemcpyAsync(dst + size_t(i) * view_raw, (const char*)images_ + size_t(used[c0 + i]) * view_raw,
+                                    view_raw, cudaMemcpyHostToDevice, s_copy_))
+                    return cuda_fail("projection upload");
+        }
+        cudaEventRecord(ev_up[slot], s_copy_);
+        cudaStreamWaitEvent(s_comp_, ev_up[slot], 0);
+        const FilterArgs fa = filter_args(det_, raw_type_, M, logM, n, store_scale);
+        cudaEventRecord(tf[2 * (c0 / chunk)], s_comp_);
+        if (filter_launch(dst, raw_type_, (char*)d_filtered_.p + size_t(c0) * view_filt, store_, fa,
+                          (const float2*)d_tw_.p, (const float*)d_K_.p, s_comp_))
+            return cuda_fail("filter launch");
+        cudaEventRecord(tf[2 * (c0 / chunk) + 1], s_comp_);
+        cudaEventRecord(ev_free[slot], s_comp_);
+        if (!in_pinned) cudaStreamSynchronize(s_copy_);
+    }
+    cudaEventRecord(e_f1, s_comp_);
+
+    // ---- backprojection per slab + layout + download
+    cudaEventRecord(e_b0, s_comp_);
+    auto host_copy = [&](int k) {
+        // pageable output: staged slab k -> final position
+        const int b = k % 2;
+        const int zb = k * slab, zs = std::min(slab, Z - zb);
+        cudaEventSynchronize(ev_down[b]);
+        const float* src = (const float*)h_stage_[b].p;
+        if (order == CTB_Z_FASTEST) {
+            parallel_for(plane, [&](size_t i) {
+                std::memcpy(out + i * Z + zb, src + i * zs, sizeof(float) * zs);
+            });
+        } else {
+            const size_t n = plane * zs;
+            const size_t parts = 16;
+            parallel_for(parts, [&](size_t p) {
+                const size_t a = p * n / parts, e = (p + 1) * n / parts;
+                std::memcpy(out + size_t(zb) * plane + a, src + a, sizeof(float) * (e - a));
+            });
+        }
+    };
+    for (int k = 0; k < nslabs; ++k) {
+        if (stop_) { cuda_fail("stop"); return fail(CTB_INTERRUPTED, "User interrupted. Stopping."); }
+        const int b = k % 2;
+        const int zb = k * slab, ze = std::min(Z, zb + slab), zs = ze - zb;
+        if (k >= 2) cudaStreamWaitEvent(s_comp_, ev_down[b], 0);
+        const ProjGeom g = proj_geom(det_, grid_, zb, ze, load_scale);
+        cudaEventRecord(tb[2 * k], s_comp_);
+        if (backproject_launch(d_filtered_.p, store_, (const float4*)d_views_.p, V, g, (float*)d_slab_[b].p, 0,
+                               s_comp_))
+            return cuda_fail("backprojection launch");
+        cudaEventRecord(tb[2 * k + 1], s_comp_);
+        const float* src = (const float*)d_slab_[b].p;
+        if (convert) {
+            if (layout_launch(src, X, Y, zs, CTB_Z_FASTEST, CTB_LITTLE_ENDIAN, d_conv_[b].p, s_comp_))
+                return cuda_fail("layout launch");
+            src = (const float*)d_conv_[b].p;
+        }
+        cudaEventRecord(ev_bp[b], s_comp_);
+        cudaStreamWaitEvent(s_down_, ev_bp[b], 0);
+        cudaError_t ce;
+        if (out_pinned) {
+            if (convert)
+                ce = cudaMemcpy2DAsync(out + zb, sizeof(float) * Z, src, sizeof(float) * zs, sizeof(float) * zs,
+                                       plane, cudaMemcpyDeviceToHost, s_down_);
+            else
+                ce = cudaMemcpyAsync(out + size_t(zb) * plane, src, sizeof(float) * plane * zs,
+                                     cudaMemcpyDeviceToHost, s_down_);
+        } else {
+            if (k >= 2) host_copy(k - 2);  // frees staging buffer b
+            ce = cudaMemcpyAsync(h_stage_[b].p, src, sizeof(float) * plane * zs, cudaMemcpyDeviceToHost, s_down_);
+        }
+        if (ce != cudaSuccess) return cuda_fail("volume download");
+        cudaEventRecord(ev_down[b], s_down_);
+        progress(1, 100.0 * double(k + 1) / double(nslabs));
+    }
+    cudaEventRecord(e_b1, s_comp_);
+    if (!out_pinned)
+        for (int k = std::max(0, nslabs - 2); k < nslabs; ++k) host_copy(k);
+    if (cudaStreamSynchronize(s_down_) != cudaSuccess || cudaStreamSynchronize(s_comp_) != cudaSuccess ||
+        cudaStreamSynchronize(s_copy_) != cudaSuccess)
+        return cuda_fail("reconstruction");
+    float phase_ms = 0, tail_ms = 0;
+    double f_ms = 0, b_ms = 0;
+    cudaEventElapsedTime(&phase_ms, e_f0, e_f1);
+    for (int i = 0; i < nchunks; ++i) { float t = 0; cudaEventElapsedTime(&t, tf[2 * i], tf[2 * i + 1]); f_ms += t; }
+    for (int i = 0; i < nslabs; ++i) { float t = 0; cudaEventElapsedTime(&t, tb[2 * i], tb[2 * i + 1]); b_ms += t; }
+    cudaEventElapsedTime(&tail_ms, e_b0, e_b1);
+    cleanup();
+    const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    tm_.filter_s = f_ms * 1e-3;
+    tm_.backproject_s = b_ms * 1e-3;
+    tm_.upload_s = std::max(0.0, (phase_ms - f_ms) * 1e-3);
+    tm_.download_s = std::max(0.0, total - (phase_ms + tail_ms) * 1e-3);
+    tm_.total_s = total;
+    tm_.voxel_views = double(X) * Y * Z * V;
+    return CTB_OK;
+}
+
+int Reconstructor::get_volume(float* host_out, int index_order) const {
+    const int X = vol_dims_[0], Y = vol_dims_[1], Z = vol_dims_[2];
+    if (X == 0 || !volume_.p) return CTB_ERR_ARG;
+    const float* v = static_cast<const float*>(volume_.p);
+    if (index_order == CTB_X_FASTEST) {
+        std::memcpy(host_out, v, sizeof(float) * size_t(X) * Y * Z);
+    } else {
+        parallel_for(size_t(X), [&](size_t x) {
+            for (int y = 0; y < Y; ++y)
+                for (int z = 0; z < Z; ++z)
+                    host_out[(x * Y + y) * Z + z] = v[(size_t(z) * Y + y) * X + x];
+        });
+    }
+    return CTB_OK;
+}
+
+}  // namespace ctb

@@ -1,0 +1,124 @@
+// Reconstruction facade: the B200 counterpart of ct::CtVolume
+// (Ct/CtVolume.h:57-278). One context drives one device.
+#pragma once
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../ctb_internal.h"
+
+namespace ctb {
+
+// Device buffer that only grows (reused across reconstructions).
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n, const char* what);
+    void release();
+    ~DevBuf() { release(); }
+};
+
+// Page-locked host buffer.
+struct HostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    bool pinned = false;
+    int ensure(size_t n);
+    void release();
+    ~HostBuf() { release(); }
+};
+
+class Reconstructor {
+   public:
+    Reconstructor();
+    ~Reconstructor();
+
+    // ---- input (sinogramFromImages and its in-memory equivalent)
+    int load_csv(const std::string& csv_path);
+    int set_projections(const void* images, int raw_type, int n_views, int width, int height,
+                        const double* angles_deg, const double* heights_mm, double pixel_size, int ccw,
+                        double u_offset_mm, double fcd_mm, double base_intensity);
+
+    // ---- settings
+    int set_bounds(float xF, float xT, float yF, float yT, float zF, float zT);
+    int set_filter(int f);
+    int set_skip(unsigned skip) { step_ = int(skip) + 1; return CTB_OK; }
+    int set_device(int d);
+    int set_spare_mb(size_t mb) { spare_mb_ = mb; return CTB_OK; }
+    int set_precision(int t);
+    int set_pad(int p);
+    int set_grid(int x, int y, int z, float vs);
+    int set_slab(int s) { slab_req_ = s; return CTB_OK; }
+    void set_progress(ctb_progress_cb cb, void* user) { cb_ = cb; cb_user_ = user; }
+
+    // ---- getters
+    const ctb_detector& detector() const { return det_; }
+    const ctb_grid& grid() const { return grid_; }
+    int views() const { return int(angles_.size()); }
+    double pixel_size() const { return pixel_size_; }
+    const ctb_timings& timings() const { return tm_; }
+
+    // ---- work
+    int reconstruct(float* host_out, int index_order);   // host_out == nullptr: keep internally
+    int get_volume(float* host_out, int index_order) const;
+    int save(const std::string& path, int index_order, int byte_order);
+    void stop() { stop_ = true; }
+
+    const std::string& error() const { return err_; }
+
+   private:
+    int fail(int status, const std::string& msg);
+    int assign_scan(const void* images, int raw_type, int n_views, int width, int height,
+                    const double* angles_deg, const double* heights_mm, double pixel_size, int ccw,
+                    double u_offset_mm, double fcd_mm, double base_intensity);
+    void update_grid();
+    int run_pipeline(float* host_out, int index_order);
+    void progress(int stage, double pct) { if (cb_) cb_(stage, pct, cb_user_); }
+
+    std::mutex mtx_;                 // exclusiveFunctionsMutex (Ct/CtVolume.h:258)
+    std::atomic<bool> stop_{false};  // stopActiveProcess (:245)
+    std::string err_;
+
+    // scan (reference members :225-232)
+    ctb_detector det_{};
+    double pixel_size_ = 0;          // stored as float by the reference
+    int raw_type_ = 0;
+    std::vector<double> angles_;     // degrees, direction-corrected
+    std::vector<double> heights_px_; // relative, in pixels
+    HostBuf images_owned_;           // decoded CSV images
+    const void* images_ = nullptr;   // V x H x W raw samples (owned or caller's)
+    bool have_scan_ = false;
+
+    // settings
+    int filter_ = CTB_RAMLAK;
+    int step_ = 1;
+    int device_ = 0;
+    size_t spare_mb_ = 200;
+    int store_ = CTB_FP32;
+    int pad_ = 1;
+    int grid_x_ = 0, grid_y_ = 0, grid_z_ = 0;
+    float grid_vs_ = 1.0f;
+    int slab_req_ = 0;
+    float rel_[6] = {0, 1, 0, 1, 0, 1};
+    ctb_progress_cb cb_ = nullptr;
+    void* cb_user_ = nullptr;
+
+    // geometry (updateBoundaries)
+    ctb_grid grid_{};
+
+    // result: X-fastest box volume in host memory
+    HostBuf volume_;
+    int vol_dims_[3] = {0, 0, 0};
+    ctb_timings tm_{};
+
+    // cached device resources
+    cudaStream_t s_copy_ = nullptr, s_comp_ = nullptr, s_down_ = nullptr;
+    DevBuf d_filtered_, d_ring_, d_views_, d_angles_, d_heights_, d_tw_, d_K_, d_slab_[2], d_conv_[2];
+    HostBuf h_stage_[2];
+    int tables_key_[3] = {-1, -1, -1};   // W, pad, filter of the cached tables
+};
+
+}  // namespace ctb

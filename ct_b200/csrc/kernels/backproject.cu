@@ -1,0 +1,185 @@
+// Kernel (c): voxel-driven FDK backprojection, and the FP64 per-view geometry.
+//
+// Reference semantics: reconstructionCore (Ct/CtVolume.cpp:923-1046, CPU, the
+// parity target) and reconstructionKernel (Ct/cuda_ct.cu:201-292, GPU):
+//   x,y,z world = index - pre            (updateBoundaries :1419-1421)
+//   cylinder    x^2 + y^2 < radius^2     (:980)
+//   t = -x sin + y cos + uOffset, s = x cos + y sin, U = D/(D - s), u = t U
+//   u in [-W/2, W-1.1-W/2]               (:998, bounds :924-925)
+//   v = (z + h) U in [1.1-H/2+..., H/2]  (:1008-1011, bounds :927-928)
+//   bilinear at (u + W/2, -v + H/2), weight U^2, vol += U^2 * value
+//
+// Design (B200): one thread owns an (x, y) column of ZC consecutive z voxels
+// and keeps their sums in registers across every view of the launch, so the
+// volume is written once per launch instead of read-modify-written per view
+// (the reference launches once per view). u, U and U^2 depend only on
+// (x, y, view) and are computed once per view for the whole column; per voxel
+// only v, the row index and the bilinear sample remain. The per-view table
+// {sin, cos, h} is built in FP64 on the device and staged into shared memory
+// once per CTA. Warps run along x, so each z row of stores is one coalesced
+// 128-byte segment of the X-fastest slab.
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "../ctb_internal.h"
+
+namespace ctb {
+
+namespace {
+
+__global__ void view_table_kernel(const double* __restrict__ ang, const double* __restrict__ h, int n,
+                                  float4* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // float angle_rad = (angle / 180.0) * M_PI; sine = sin(angle_rad) (:953-955)
+    const float angle_rad = float((ang[i] / 180.0) * 3.14159265358979323846);
+    double s, c;
+    sincos(double(angle_rad), &s, &c);
+    out[i] = make_float4(float(s), float(c), float(h[i]), 0.0f);
+}
+
+template <typename T> __device__ __forceinline__ float ld(const T* p);
+template <> __device__ __forceinline__ float ld<float>(const float* p) { return __ldg(p); }
+template <> __device__ __forceinline__ float ld<__half>(const __half* p) { return __half2float(__ldg(p)); }
+template <> __device__ __forceinline__ float ld<__nv_bfloat16>(const __nv_bfloat16* p) {
+    return __bfloat162float(__ldg(p));
+}
+
+constexpr int kBX = 32, kBY = 4;
+constexpr int kViewsPerStage = 1024;   // shared-memory view table capacity (16 KB)
+
+template <typename T, int ZC>
+__global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ proj,
+                                                       const float4* __restrict__ views, int n_views,
+                                                       ProjGeom g, float* __restrict__ vol, int accumulate) {
+    __shared__ float4 sviews[kViewsPerStage];
+    const int x = blockIdx.x * kBX + threadIdx.x;
+    const int y = blockIdx.y * kBY + threadIdx.y;
+    const int z0 = blockIdx.z * ZC;
+    const int tid = threadIdx.y * kBX + threadIdx.x;
+
+    const float xw = (float(x) - g.xPre) * g.vs;
+    const float yw = (float(y) - g.yPre) * g.vs;
+    const bool live = x < g.X && y < g.Y && (xw * xw + yw * yw) < g.r2;
+    // (z - zPre) is exact for every z; rounding happens once, in the product
+    // with the voxel pitch, exactly as the forward projector evaluates it.
+    const float zr0 = float(z0) - g.zPre;
+
+    float acc[ZC];
+#pragma unroll
+    for (int j = 0; j < ZC; ++j) acc[j] = 0.0f;
+
+    for (int vb = 0; vb < n_views; vb += kViewsPerStage) {
+        const int nv = min(kViewsPerStage, n_views - vb);
+        __syncthreads();
+        for (int i = tid; i < nv; i += kBX * kBY) sviews[i] = __ldg(&views[vb + i]);
+        __syncthreads();
+        if (!live) continue;
+        const T* pv = proj + (long long)vb * g.view_stride;
+        for (int iv = 0; iv < nv; ++iv, pv += g.view_stride) {
+            const float4 q = sviews[iv];  // sin, cos, h
+            float t = (-1) * xw * q.x + yw * q.y;
+            t += g.uOff;
+            const float s = xw * q.y + yw * q.x;
+            const float U = g.D / (g.D - s);
+            const float u = t * U;
+            if (!(u >= g.lbU && u <= g.ubU)) continue;
+            const float w = U * U * g.load_scale;
+            const float ui = u + g.uPre;
+            const int u0 = int(ui);
+            const float fu = ui - float(u0);
+            const T* col = pv + u0;
+#pragma unroll
+            for (int j = 0; j < ZC; ++j) {
+                const float zw = (zr0 + float(j)) * g.vs;
+                const float v = (zw + q.z) * U;
+                if (v >= g.lbV && v <= g.ubV) {
+                    const float vi = (-1) * v + g.vPre;
+                    const int v0 = int(vi);
+                    const float fv = vi - float(v0);
+                    const T* r0 = col + (long long)v0 * g.W;
+                    const float a = (1.0f - fu) * ld(r0) + fu * ld(r0 + 1);
+                    const float b = (1.0f - fu) * ld(r0 + g.W) + fu * ld(r0 + g.W + 1);
+                    acc[j] += w * ((1.0f - fv) * a + fv * b);
+                }
+            }
+        }
+    }
+    if (x >= g.X || y >= g.Y) return;
+    const long long plane = (long long)g.X * g.Y;
+    float* out = vol + (long long)z0 * plane + (long long)y * g.X + x;
+#pragma unroll
+    for (int j = 0; j < ZC; ++j) {
+        if (z0 + j < g.Zs) {
+            float* p = out + j * plane;
+            *p = accumulate ? (*p + acc[j]) : acc[j];
+        }
+    }
+}
+
+template <typename T>
+int bp_launch_typed(const T* proj, const float4* views, int n_views, const ProjGeom& g, float* vol,
+                    int accumulate, cudaStream_t s) {
+    constexpr int ZC = 16;
+    dim3 block(kBX, kBY, 1);
+    dim3 grid((g.X + kBX - 1) / kBX, (g.Y + kBY - 1) / kBY, (g.Zs + ZC - 1) / ZC);
+    if (grid.x == 0 || grid.y == 0 || grid.z == 0) return CTB_OK;
+    if (grid.z > 65535 || grid.y > 65535) {
+        set_global_error("backproject: grid too large");
+        return CTB_ERR_UNSUPPORTED;
+    }
+    bp_kernel<T, ZC><<<grid, block, 0, s>>>(proj, views, n_views, g, vol, accumulate);
+    return cuda_status(cudaGetLastError(), "bp_kernel launch");
+}
+
+}  // namespace
+
+int view_table_build(const double* angles_deg_dev, const double* heights_dev, int n, float4* out,
+                     cudaStream_t s) {
+    if (n <= 0) return CTB_OK;
+    view_table_kernel<<<(n + 127) / 128, 128, 0, s>>>(angles_deg_dev, heights_dev, n, out);
+    return cuda_status(cudaGetLastError(), "view_table_kernel launch");
+}
+
+ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_end, float load_scale) {
+    ProjGeom g;
+    g.W = det.width;
+    g.H = det.height;
+    g.X = grid.x_to - grid.x_from;
+    g.Y = grid.y_to - grid.y_from;
+    g.Zs = z_end - z_begin;
+    // updateBoundaries :1419-1423 (double expressions stored as float)
+    g.xPre = float(float(grid.x_size) / 2.0 - float(grid.x_from));
+    g.yPre = float(float(grid.y_size) / 2.0 - float(grid.y_from));
+    const float zPre = float(float(grid.z_size) / 2.0 - float(grid.z_from));
+    g.zPre = zPre - float(z_begin);
+    g.vs = grid.voxel_pitch;
+    g.D = det.fcd;
+    g.uOff = det.u_offset;
+    g.r2 = det.radius * det.radius;
+    g.uPre = float(double(det.width) / 2.0);
+    g.vPre = float(double(det.height) / 2.0);
+    // reconstructionCore :924-928
+    g.lbU = 0.0f - g.uPre;
+    g.ubU = float(double(det.width) - 1 - 0.1) - g.uPre;
+    g.lbV = (-1) * float(double(det.height) - 1 - 0.1) + g.vPre;
+    g.ubV = (-1) * 0.0f + g.vPre;
+    g.load_scale = load_scale;
+    g.view_stride = (long long)det.width * det.height;
+    return g;
+}
+
+int backproject_launch(const void* proj, int store_type, const float4* views, int n_views,
+                       const ProjGeom& g, float* vol, int accumulate, cudaStream_t s) {
+    switch (store_type) {
+        case CTB_FP32: return bp_launch_typed((const float*)proj, views, n_views, g, vol, accumulate, s);
+        case CTB_FP16: return bp_launch_typed((const __half*)proj, views, n_views, g, vol, accumulate, s);
+        case CTB_BF16:
+            return bp_launch_typed((const __nv_bfloat16*)proj, views, n_views, g, vol, accumulate, s);
+    }
+    set_global_error("backproject: unknown storage type");
+    return CTB_ERR_ARG;
+}
+
+}  // namespace ctb

@@ -1,0 +1,156 @@
+"""CtVolume: the reference's reconstruction facade (Ct/CtVolume.h:57-278) over libctb.
+
+Method names and argument meanings follow ct::CtVolume; errors raise CtbError
+carrying the message the reference would have emitted with
+CompletionStatus::error (user interruption raises with status INTERRUPTED).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check, lib
+
+FILTER_NAMES = {"ramlak": L.RAMLAK, "shepplogan": L.SHEPPLOGAN, "hann": L.HANN}
+RAW_TYPES = {np.dtype(np.uint8): L.U8, np.dtype(np.uint16): L.U16, np.dtype(np.float32): L.F32}
+
+
+class CtVolume:
+    def __init__(self, csv_file: str | None = None):
+        self._ctx = ctypes.c_void_p()
+        check(lib().ctb_create(ctypes.byref(self._ctx)))
+        self._keep = None
+        self._cb = None
+        if csv_file is not None:
+            self.sinogramFromImages(csv_file)
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx is not None and ctx.value and L._lib is not None:
+            L._lib.ctb_destroy(ctx)
+            self._ctx = None
+
+    def _ck(self, status):
+        return check(status, self._ctx)
+
+    # ---------------------------------------------------------------- input
+    def sinogramFromImages(self, csv_file: str) -> bool:
+        self._ck(lib().ctb_load_csv(self._ctx, str(csv_file).encode()))
+        return True
+
+    def setProjections(self, images: np.ndarray, angles_deg, height_offsets_mm=None, *, pixel_size: float,
+                       rotation: str = "ccw", u_offset_mm: float = 0.0, fcd_mm: float, base_intensity: float = 1.0):
+        """In-memory equivalent of sinogramFromImages: images (V, H, W) uint8/uint16/float32 in host memory."""
+        images = np.ascontiguousarray(images)
+        V, H, W = images.shape
+        a = np.ascontiguousarray(angles_deg, np.float64)
+        h = None if height_offsets_mm is None else np.ascontiguousarray(height_offsets_mm, np.float64)
+        ccw = {"ccw": 1, "cw": 0}.get(rotation, -1)
+        self._ck(lib().ctb_set_projections(self._ctx, images.ctypes.data, RAW_TYPES[images.dtype], V, W, H,
+                                           a.ctypes.data, None if h is None else h.ctypes.data, pixel_size, ccw,
+                                           u_offset_mm, fcd_mm, base_intensity))
+        self._keep = images  # the context reads the images during reconstruction
+
+    def setProjectionsPointer(self, ptr: int, raw_type: int, n_views: int, width: int, height: int, angles_deg,
+                              height_offsets_mm=None, *, pixel_size: float, rotation: str = "ccw",
+                              u_offset_mm: float = 0.0, fcd_mm: float, base_intensity: float = 1.0, keep=None):
+        """Like setProjections for a raw host pointer (e.g. a pinned torch tensor's data_ptr())."""
+        a = np.ascontiguousarray(angles_deg, np.float64)
+        h = None if height_offsets_mm is None else np.ascontiguousarray(height_offsets_mm, np.float64)
+        ccw = {"ccw": 1, "cw": 0}.get(rotation, -1)
+        self._ck(lib().ctb_set_projections(self._ctx, ptr, raw_type, n_views, width, height, a.ctypes.data,
+                                           None if h is None else h.ctypes.data, pixel_size, ccw, u_offset_mm,
+                                           fcd_mm, base_intensity))
+        self._keep = keep
+
+    # ------------------------------------------------------------- settings
+    def setVolumeBounds(self, xFrom, xTo, yFrom, yTo, zFrom, zTo):
+        self._ck(lib().ctb_set_volume_bounds(self._ctx, xFrom, xTo, yFrom, yTo, zFrom, zTo))
+
+    def setFrequencyFilterType(self, filter_type):
+        if isinstance(filter_type, str):
+            filter_type = FILTER_NAMES.get(filter_type.lower(), L.RAMLAK)
+        self._ck(lib().ctb_set_filter(self._ctx, int(filter_type)))
+
+    def setSkipProjections(self, value: int = 0):
+        self._ck(lib().ctb_set_skip_projections(self._ctx, value))
+
+    def setActiveCudaDevices(self, devices):
+        self._ck(lib().ctb_set_device(self._ctx, int(list(devices)[0])))
+
+    def setGpuSpareMemory(self, megabytes: int):
+        self._ck(lib().ctb_set_gpu_spare_memory(self._ctx, int(megabytes)))
+
+    def setPrecision(self, store: str | int):
+        t = {"fp32": L.FP32, "fp16": L.FP16, "bf16": L.BF16}.get(store, store) if isinstance(store, str) else store
+        self._ck(lib().ctb_set_precision(self._ctx, int(t)))
+
+    def setPad(self, pad: int):
+        self._ck(lib().ctb_set_pad(self._ctx, int(pad)))
+
+    def setGrid(self, x: int, y: int, z: int, voxel_pitch: float):
+        self._ck(lib().ctb_set_grid(self._ctx, x, y, z, voxel_pitch))
+
+    def setSlabHeight(self, slices: int):
+        self._ck(lib().ctb_set_slab_height(self._ctx, slices))
+
+    def setProgressCallback(self, fn):
+        """fn(stage, percent); stage 0 loading, 1 reconstruction, 2 saving."""
+        self._cb = L.PROGRESS_CB(lambda s, p, u: fn(s, p)) if fn else L.PROGRESS_CB()
+        self._ck(lib().ctb_set_progress_callback(self._ctx, self._cb, None))
+
+    # --------------------------------------------------------------- getters
+    def detector(self) -> L.Detector:
+        d = L.Detector()
+        self._ck(lib().ctb_get_detector(self._ctx, ctypes.byref(d)))
+        return d
+
+    def grid(self) -> L.Grid:
+        g = L.Grid()
+        self._ck(lib().ctb_get_grid(self._ctx, ctypes.byref(g)))
+        return g
+
+    def getXSize(self): return self.grid().box[0]
+    def getYSize(self): return self.grid().box[1]
+    def getZSize(self): return self.grid().box[2]
+    def getImageWidth(self): return self.detector().width
+    def getImageHeight(self): return self.detector().height
+    def getFCD(self): return self.detector().fcd
+    def getUOffset(self): return self.detector().u_offset
+    def getBaseIntensity(self): return self.detector().base_intensity
+    def getPixelSize(self): return lib().ctb_get_pixel_size(self._ctx)
+    def getReconstructionCylinderRadius(self): return int(self.detector().radius)
+
+    def getSinogramSize(self) -> int:
+        n = ctypes.c_int()
+        self._ck(lib().ctb_get_sinogram_size(self._ctx, ctypes.byref(n)))
+        return n.value
+
+    # ------------------------------------------------------------------ work
+    def reconstructVolume(self):
+        self._ck(lib().ctb_reconstruct(self._ctx))
+
+    def reconstructInto(self, out_ptr: int, index_order: int = L.X_FASTEST):
+        """Reconstruct into caller host memory (pinned memory is written without staging)."""
+        self._ck(lib().ctb_reconstruct_into(self._ctx, out_ptr, index_order))
+
+    def volume(self, index_order: int = L.X_FASTEST) -> np.ndarray:
+        """The last reconstructed volume: shape (Z, Y, X) for X_FASTEST, (X, Y, Z) for Z_FASTEST."""
+        x, y, z = self.grid().box
+        shape = (z, y, x) if index_order == L.X_FASTEST else (x, y, z)
+        out = np.empty(shape, np.float32)
+        self._ck(lib().ctb_get_volume(self._ctx, out.ctypes.data, index_order))
+        return out
+
+    def saveVolumeToBinaryFile(self, filename: str, indexOrder: int = L.Z_FASTEST, byteOrder: int = L.LITTLE_ENDIAN):
+        self._ck(lib().ctb_save_volume(self._ctx, str(filename).encode(), indexOrder, byteOrder))
+
+    def stop(self):
+        lib().ctb_stop(self._ctx)
+
+    def timings(self) -> L.Timings:
+        t = L.Timings()
+        self._ck(lib().ctb_get_timings(self._ctx, ctypes.byref(t)))
+        return t

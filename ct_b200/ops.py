@@ -1,0 +1,123 @@
+"""Operator layer over device memory (torch tensors as plain device buffers).
+
+These mirror the reference's kernel API (Ct/cuda_ct.h:18-69): callers own the
+device memory and pass a stream; the functions enqueue work and return.
+torch is only used for allocation, streams and pointers.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check, lib
+
+STORE_DTYPES = {}
+RAW_CODES = {}
+
+
+def _torch():
+    import torch
+    if not STORE_DTYPES:
+        STORE_DTYPES.update({L.FP32: torch.float32, L.FP16: torch.float16, L.BF16: torch.bfloat16})
+        RAW_CODES.update({torch.uint8: L.U8, torch.uint16: L.U16, torch.float32: L.F32})
+    return torch
+
+
+def _stream(stream):
+    torch = _torch()
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+def detector(width, height, fcd, u_offset=0.0, base_intensity=1.0, rel=None):
+    """Detector record plus the reference grid (radius, grid rule, bounds)."""
+    d = L.Detector(width, height, fcd, u_offset, base_intensity, 0.0)
+    g = L.Grid()
+    r = None if rel is None else (ctypes.c_float * 6)(*rel)
+    check(lib().ctb_reference_grid(ctypes.byref(d), r, ctypes.byref(g)))
+    return d, g
+
+
+def custom_grid(d: L.Detector, size, voxel_pitch, box=None) -> L.Grid:
+    x, y, z = size
+    if box is None:
+        box = (0, x, 0, y, 0, z)
+    return L.Grid(x, y, z, *box, voxel_pitch)
+
+
+def filter_projections(raw, det: L.Detector, filter_type=L.RAMLAK, pad=1, store=L.FP32, store_scale=1.0,
+                       out=None, stream=None):
+    """raw: (V, H, W) uint8/uint16/float32 CUDA tensor -> filtered (V, H, W) in the storage dtype."""
+    torch = _torch()
+    assert raw.is_cuda and raw.is_contiguous()
+    V = raw.shape[0]
+    if out is None:
+        out = torch.empty(raw.shape, dtype=STORE_DTYPES[store], device=raw.device)
+    check(lib().ctb_filter_projections(ctypes.c_void_p(raw.data_ptr()), RAW_CODES[raw.dtype], V, ctypes.byref(det),
+                                       filter_type, pad, ctypes.c_void_p(out.data_ptr()), store, store_scale,
+                                       _stream(stream)))
+    return out
+
+
+def backproject(filtered, angles_deg, heights_px, det: L.Detector, grid: L.Grid, z_begin=0, z_end=None,
+                load_scale=1.0, out=None, accumulate=False, stream=None):
+    """Filtered projections (V, H, W) -> X-fastest slab (Zs, Y, X) float32."""
+    torch = _torch()
+    store = {v: k for k, v in STORE_DTYPES.items()}[filtered.dtype]
+    X, Y, Z = grid.box
+    if z_end is None:
+        z_end = Z
+    if out is None:
+        out = torch.empty((z_end - z_begin, Y, X), dtype=torch.float32, device=filtered.device)
+    a = np.ascontiguousarray(angles_deg, np.float64)
+    h = np.ascontiguousarray(heights_px if heights_px is not None else np.zeros_like(a), np.float64)
+    check(lib().ctb_backproject(ctypes.c_void_p(filtered.data_ptr()), store, len(a), a.ctypes.data, h.ctypes.data,
+                                ctypes.byref(det), ctypes.byref(grid), z_begin, z_end, load_scale,
+                                ctypes.c_void_p(out.data_ptr()), int(accumulate), _stream(stream)))
+    return out
+
+
+def forward_project(vol, angles_deg, heights_px, det: L.Detector, grid: L.Grid, z_begin=0, z_end=None, out=None,
+                    accumulate=False, stream=None):
+    """X-fastest slab (Zs, Y, X) float32 -> projections (V, H, W) float32 (transpose of backproject)."""
+    torch = _torch()
+    X, Y, Z = grid.box
+    if z_end is None:
+        z_end = Z
+    a = np.ascontiguousarray(angles_deg, np.float64)
+    h = np.ascontiguousarray(heights_px if heights_px is not None else np.zeros_like(a), np.float64)
+    if out is None:
+        out = torch.empty((len(a), det.height, det.width), dtype=torch.float32, device=vol.device)
+    check(lib().ctb_forward_project(ctypes.c_void_p(vol.data_ptr()), a.ctypes.data, h.ctypes.data, len(a),
+                                    ctypes.byref(det), ctypes.byref(grid), z_begin, z_end,
+                                    ctypes.c_void_p(out.data_ptr()), int(accumulate), _stream(stream)))
+    return out
+
+
+def convert_layout(src, index_order, byte_order=L.LITTLE_ENDIAN, out=None, stream=None):
+    """X-fastest slab (Zs, Y, X) -> same bytes in index_order / byte_order (returned as int32 view if swapped)."""
+    torch = _torch()
+    zs, y, x = src.shape
+    if out is None:
+        out = torch.empty(src.numel(), dtype=torch.float32, device=src.device)
+    check(lib().ctb_convert_layout(ctypes.c_void_p(src.data_ptr()), x, y, zs, index_order, byte_order,
+                                   ctypes.c_void_p(out.data_ptr()), _stream(stream)))
+    return out
+
+
+def phantom_project(ellipsoids, angles_deg, heights_mm, width, height, pixel_mm, fcd_mm, u_offset_mm=0.0,
+                    out=None, device="cuda", stream=None):
+    """Analytic line integrals (FP64, device) of an (n, 16) ellipsoid table -> (V, H, W) float64."""
+    torch = _torch()
+    e = torch.as_tensor(np.ascontiguousarray(ellipsoids, np.float64), device=device)
+    a = np.ascontiguousarray(angles_deg, np.float64)
+    h = None if heights_mm is None else np.ascontiguousarray(heights_mm, np.float64)
+    if out is None:
+        out = torch.empty((len(a), height, width), dtype=torch.float64, device=device)
+    check(lib().ctb_phantom_project(ctypes.c_void_p(e.data_ptr()), e.shape[0], a.ctypes.data,
+                                    None if h is None else h.ctypes.data, len(a), width, height, pixel_mm, fcd_mm,
+                                    u_offset_mm, ctypes.c_void_p(out.data_ptr()), _stream(stream)))
+    return out

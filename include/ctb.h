@@ -1,0 +1,244 @@
+/*
+ * ctb.h -- C ABI of the B200 FDK cone-beam reconstruction engine.
+ *
+ * Two layers, mirroring the two layers of the reference (bastian-weber/Ct):
+ *
+ *  1. Operator layer (device pointers + a CUDA stream), replacing the
+ *     reference's kernel API in Ct/cuda_ct.h:18-69 and the OpenCV/cuFFT glue in
+ *     Ct/CtVolume.cpp:887-921.  Callers own all device memory they pass.
+ *
+ *  2. Reconstruction facade (opaque context), replacing the public surface of
+ *     ct::CtVolume (Ct/CtVolume.h:63-121): load the CSV + images, set bounds and
+ *     filter, reconstruct, save.  The context owns its device memory.
+ *
+ * Conventions
+ *  - Every function returns an int status (CTB_OK == 0) unless stated; a
+ *    human-readable message for the last failure is kept per context
+ *    (ctb_last_error) or per thread for context-free calls
+ *    (ctb_last_error_global).  No C++ exception crosses this boundary.
+ *    Reference: bool& success out-params + lastErrorMessage +
+ *    CompletionStatus (Ct/cuda_ct.cu:95-99, Ct/CtVolume.h:260, Common/types.h:11-20).
+ *  - Units follow the reference: detector coordinates in pixels of the virtual
+ *    detector at the rotation axis (CSV pixel size), FCD and uOffset divided by
+ *    the pixel size (Ct/CtVolume.cpp:170-172), angles in degrees.
+ *  - Volumes on the device are X-fastest (idx = z*X*Y + y*X + x), as the
+ *    reference's GPU path (Ct/cuda_ct.cu:193-199).
+ *  - cudaStream_t is passed as void* so this header needs no CUDA include.
+ */
+#ifndef CTB_H
+#define CTB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+enum {
+    CTB_OK = 0,
+    CTB_ERR_ARG = 1,         /* invalid argument / state */
+    CTB_ERR_IO = 2,          /* file could not be opened, read or written */
+    CTB_ERR_CSV = 3,         /* configuration file could not be parsed */
+    CTB_ERR_IMAGE = 4,       /* image missing, unsupported depth or size mismatch */
+    CTB_ERR_ALLOC = 5,       /* device or pinned host allocation failed */
+    CTB_ERR_CUDA = 6,        /* CUDA runtime error */
+    CTB_ERR_TIMEOUT = 7,     /* a bounded device wait gave up */
+    CTB_INTERRUPTED = 8,     /* ctb_stop() was called (CompletionStatus::interrupted) */
+    CTB_ERR_UNSUPPORTED = 9  /* size or option beyond what this build supports */
+};
+
+/* FilterType, Ct/CtVolume.h:50-54 (same numeric values). */
+enum { CTB_RAMLAK = 0, CTB_SHEPPLOGAN = 1, CTB_HANN = 2 };
+
+/* IndexOrder, Common/Volume.h:29-32. */
+enum { CTB_X_FASTEST = 0, CTB_Z_FASTEST = 1 };
+
+/* QDataStream::ByteOrder as used by saveVolumeToBinaryFile. */
+enum { CTB_LITTLE_ENDIAN = 0, CTB_BIG_ENDIAN = 1 };
+
+/* Storage type of raw / filtered projections; arithmetic is always FP32. */
+enum { CTB_FP32 = 0, CTB_FP16 = 1, CTB_BF16 = 2 };
+
+/* Raw projection pixel types accepted (cv::imread depths the reference accepts,
+ * Ct/CtVolume.cpp:247). */
+enum { CTB_U8 = 8, CTB_U16 = 16, CTB_F32 = 32 };
+
+/* -------------------------------------------------------- geometry records */
+
+/* Per-scan detector/orbit geometry in reference units. */
+typedef struct {
+    int32_t width;          /* W, detector columns */
+    int32_t height;         /* H, detector rows */
+    float fcd;              /* focus-centre distance in pixels (CSV FCD / pixelSize) */
+    float u_offset;         /* rotation axis offset in pixels (CSV uOffset / pixelSize) */
+    float base_intensity;   /* air intensity (CSV line 6), normalised scale */
+    float radius;           /* reconstruction cylinder radius in pixels */
+} ctb_detector;
+
+/* Reconstructed box inside the full grid, plus the voxel pitch. The reference
+ * grid is xSize = ySize = 2*radius, zSize = H, voxel pitch 1 pixel
+ * (Ct/CtVolume.cpp:311-316); from/to follow updateBoundaries (:1399-1409). */
+typedef struct {
+    int32_t x_size, y_size, z_size;          /* full grid */
+    int32_t x_from, x_to, y_from, y_to, z_from, z_to;  /* box, half-open */
+    float voxel_pitch;                       /* voxel edge in detector pixels (1 = reference) */
+} ctb_grid;
+
+/* ------------------------------------------------------- operator layer */
+
+/* Device queries, Ct/cuda_ct.h:18-23. */
+int ctb_device_count(int* count);
+int ctb_device_name(int device, char* buf, size_t buf_len);
+int ctb_free_memory(int device, size_t* free_bytes, size_t* total_bytes);
+
+/* Reference grid for a detector (grid rule Ct/CtVolume.cpp:311-316 and
+ * cylinder radius :370-373) with relative bounds rel6 = {xmin,xmax,ymin,ymax,
+ * zmin,zmax} clamped like setVolumeBounds (:487-500). det->radius is set. */
+int ctb_reference_grid(ctb_detector* det, const float rel6[6], ctb_grid* grid);
+
+/* Preprocess and ramp-filter n_views raw projections in one launch sequence:
+ * -ln of the normalised intensity, Feldkamp cosine weight, and the row-wise
+ * ramp filter (ramlak / shepplogan / hann) applied in frequency with the
+ * reference's window sampling. Replaces cudaPreprocessImage
+ * (Ct/CtVolume.cpp:887-921) = convertTo/log/multiply + applyFeldkampWeightFiltering
+ * (Ct/cuda_ct.h:28-33) + cuFFT R2C + applyFrequencyFiltering (Ct/cuda_ct.h:24-27)
+ * + cuFFT C2R.
+ *   raw:       device, n_views x H x W of raw_type (CTB_U8/U16/F32), dense.
+ *   filtered:  device, n_views x H x W of store_type (CTB_FP32/FP16/BF16).
+ *   pad:       1 = reference-exact circular filter of length W (no padding);
+ *              2 = linear filter zero-padded to the next power of two >= 2W.
+ *   store_scale: filtered values are multiplied by this before storage
+ *              (1 for FP32; FP16/BF16 use a scale that keeps values near 1). */
+int ctb_filter_projections(const void* raw, int raw_type, int n_views, const ctb_detector* det,
+                           int filter, int pad, void* filtered, int store_type, float store_scale,
+                           void* stream);
+
+/* Voxel-driven FDK backprojection of n_views filtered projections into the
+ * z-slab [z_begin, z_end) of the box (indices relative to grid->z_from),
+ * X-fastest, slab-local: vol[(z - z_begin)*X*Y + y*X + x].
+ * Replaces startReconstruction / reconstructionKernel (Ct/cuda_ct.h:47-69,
+ * Ct/cuda_ct.cu:201-352), which adds one view per launch into a pitched chunk.
+ *   angles_deg / height_offsets_px: host arrays (n_views), after the
+ *     reference's direction correction and relative height offsets.
+ *   load_scale: multiplies every sample (1/store_scale of the filter).
+ *   accumulate: 0 = overwrite the slab, 1 = add to it. */
+int ctb_backproject(const void* filtered, int store_type, int n_views, const double* angles_deg,
+                    const double* height_offsets_px, const ctb_detector* det, const ctb_grid* grid,
+                    int z_begin, int z_end, float load_scale, float* vol, int accumulate, void* stream);
+
+/* Matched forward projector: the exact transpose of ctb_backproject with
+ * load_scale = 1 (same bilinear footprint, U^2 weight, cylinder and bounds
+ * masks). Input slab as ctb_backproject's output; output n_views x H x W FP32
+ * projections (overwritten when accumulate == 0). No counterpart in the
+ * reference (which has no forward model). */
+int ctb_forward_project(const float* vol, const double* angles_deg, const double* height_offsets_px,
+                        int n_views, const ctb_detector* det, const ctb_grid* grid, int z_begin,
+                        int z_end, float* proj, int accumulate, void* stream);
+
+/* Convert an X-fastest device slab (X x Y x Zs floats) into the requested
+ * index order and byte order, into dst (device). Replaces the layout/byte-order
+ * walk of Volume::saveToBinaryFile (Common/Volume.h:476-574) for one slab;
+ * for Z_FASTEST the slab is written with row length zs (the caller scatters
+ * slabs into the full z extent). */
+int ctb_convert_layout(const float* src, int x, int y, int zs, int index_order, int byte_order,
+                       void* dst, void* stream);
+
+/* ------------------------------------------------------ facade layer */
+
+typedef struct ctb_ctx ctb_ctx;
+
+/* Progress callback: stage 0 = loading, 1 = reconstruction, 2 = saving;
+ * percent 0..100 (Ct/CtVolume.h:271-276 signals). Fires on the calling thread. */
+typedef void (*ctb_progress_cb)(int stage, double percent, void* user);
+
+int ctb_create(ctb_ctx** ctx);                 /* CtVolume() */
+void ctb_destroy(ctb_ctx* ctx);
+const char* ctb_last_error(const ctb_ctx* ctx);
+const char* ctb_last_error_global(void);
+
+/* sinogramFromImages (Ct/CtVolume.cpp:136-330): parse the CSV, decode and
+ * validate every image (8/16-bit PGM or TIFF, 32-bit float TIFF), apply the
+ * direction correction and relative height offsets, set the reference grid. */
+int ctb_load_csv(ctb_ctx* ctx, const char* csv_path);
+
+/* In-memory equivalent of ctb_load_csv for callers that already hold the
+ * images: n_views raw images (raw_type) of width x height, host memory (pinned
+ * or pageable), angles in degrees and height offsets in mm exactly as they
+ * would appear in the CSV, plus the CSV header values. */
+int ctb_set_projections(ctb_ctx* ctx, const void* host_images, int raw_type, int n_views, int width,
+                        int height, const double* angles_deg, const double* height_offsets_mm,
+                        double pixel_size, int ccw, double u_offset_mm, double fcd_mm,
+                        double base_intensity);
+
+int ctb_set_volume_bounds(ctb_ctx* ctx, float xmin, float xmax, float ymin, float ymax, float zmin,
+                          float zmax);        /* setVolumeBounds */
+int ctb_set_filter(ctb_ctx* ctx, int filter);             /* setFrequencyFilterType */
+int ctb_set_skip_projections(ctb_ctx* ctx, unsigned skip);  /* setSkipProjections */
+int ctb_set_device(ctb_ctx* ctx, int device);             /* setActiveCudaDevices({d}) */
+int ctb_set_gpu_spare_memory(ctb_ctx* ctx, size_t megabytes);  /* setGpuSpareMemory */
+/* Engine extensions (no reference counterpart). */
+int ctb_set_precision(ctb_ctx* ctx, int store_type);      /* CTB_FP32 / FP16 / BF16 */
+int ctb_set_pad(ctb_ctx* ctx, int pad);                   /* 1 (reference) or 2 */
+/* Override the grid: x_size,y_size,z_size voxels of voxel_pitch detector
+ * pixels, centred like the reference grid; bounds apply on top. 0 restores the
+ * reference grid. */
+int ctb_set_grid(ctb_ctx* ctx, int x_size, int y_size, int z_size, float voxel_pitch);
+int ctb_set_slab_height(ctb_ctx* ctx, int slices);        /* 0 = automatic */
+int ctb_set_progress_callback(ctb_ctx* ctx, ctb_progress_cb cb, void* user);
+
+/* Getters (Ct/CtVolume.h:69-94). */
+int ctb_get_detector(const ctb_ctx* ctx, ctb_detector* det);
+int ctb_get_grid(const ctb_ctx* ctx, ctb_grid* grid);
+int ctb_get_volume_size(const ctb_ctx* ctx, int* x, int* y, int* z); /* getX/Y/ZSize */
+int ctb_get_sinogram_size(const ctb_ctx* ctx, int* n);
+double ctb_get_pixel_size(const ctb_ctx* ctx);
+
+/* reconstructVolume (Ct/CtVolume.cpp:543-632). The volume stays in host
+ * memory owned by the context (X-fastest) until the next call. */
+int ctb_reconstruct(ctb_ctx* ctx);
+
+/* Reconstruct straight into a caller buffer of x*y*z floats in index_order
+ * (host memory, pinned buffers are used without staging). */
+int ctb_reconstruct_into(ctb_ctx* ctx, float* host_volume, int index_order);
+
+/* Copy the last reconstructed volume into a caller buffer in index_order. */
+int ctb_get_volume(const ctb_ctx* ctx, float* host_volume, int index_order);
+
+/* saveVolumeToBinaryFile (Ct/CtVolume.cpp:634-721): <base>.txt info file,
+ * <base>.vgi header, raw float32 in index_order / byte_order. */
+int ctb_save_volume(ctb_ctx* ctx, const char* path, int index_order, int byte_order);
+
+/* stop() (Ct/CtVolume.cpp:723-726): thread-safe, polled per slab / view group. */
+void ctb_stop(ctb_ctx* ctx);
+
+/* Stage timings of the last ctb_reconstruct* call (seconds, CUDA events and
+ * steady clock). */
+typedef struct {
+    double upload_s;        /* host->device copies not hidden behind filtering */
+    double filter_s;        /* preprocessing + ramp filter kernels */
+    double backproject_s;   /* backprojection kernels */
+    double download_s;      /* device->host copies not hidden behind backprojection */
+    double total_s;         /* wall time of the whole call */
+    double voxel_views;     /* x*y*z*views processed */
+} ctb_timings;
+int ctb_get_timings(const ctb_ctx* ctx, ctb_timings* t);
+
+/* ------------------------------------------------------ synthetic data */
+
+/* Analytic line integrals of a sum of ellipsoids (test phantoms), one value
+ * per detector pixel, FP64 on the device. ellipsoids: n x 16 doubles
+ * {cx,cy,cz, a,b,c, R00..R22 (row-major rotation, body->world), density} in
+ * mm; geometry as the reference model with source-axis distance fcd_mm and
+ * detector pitch pixel_mm at the axis. out: device, n_views x H x W doubles. */
+int ctb_phantom_project(const double* ellipsoids_dev, int n_ellipsoids, const double* angles_deg,
+                        const double* height_offsets_mm, int n_views, int width, int height,
+                        double pixel_mm, double fcd_mm, double u_offset_mm, double* out_dev,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTB_H */

@@ -1,0 +1,209 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes wrapper of the CPU oracle (ct_oracle.cpp).
+
+The oracle restates the reference's CPU FDK path (bastian-weber/Ct,
+Ct/CtVolume.cpp:802-1054) in C++ and adds a double-precision version of the
+same mathematics. Only tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline leg use this module, as the checker; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libct_oracle.so")
+
+RAMLAK, SHEPPLOGAN, HANN = 0, 1, 2
+FILTERS = {"ramlak": RAMLAK, "shepplogan": SHEPPLOGAN, "hann": HANN}
+
+
+class OrcGeom(ctypes.Structure):
+    _fields_ = [
+        ("W", ctypes.c_int), ("H", ctypes.c_int),
+        ("FCD", ctypes.c_float), ("uOffset", ctypes.c_float), ("radius", ctypes.c_float),
+        ("xSize", ctypes.c_int), ("ySize", ctypes.c_int), ("zSize", ctypes.c_int),
+        ("xFrom", ctypes.c_int), ("xTo", ctypes.c_int),
+        ("yFrom", ctypes.c_int), ("yTo", ctypes.c_int),
+        ("zFrom", ctypes.c_int), ("zTo", ctypes.c_int),
+        ("vs", ctypes.c_float),
+    ]
+
+    @property
+    def box(self):
+        return (self.xTo - self.xFrom, self.yTo - self.yFrom, self.zTo - self.zFrom)
+
+
+def build() -> str:
+    """Compile the oracle library with its Makefile (g++, OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        P = ctypes.c_void_p
+        L.orc_ref_cylinder_radius.restype = ctypes.c_uint
+        L.orc_ref_cylinder_radius.argtypes = [ctypes.c_int, ctypes.c_float]
+        L.orc_ref_clamp_bounds.restype = ctypes.c_int
+        L.orc_ref_clamp_bounds.argtypes = [ctypes.c_float] * 6 + [P]
+        L.orc_ref_geom.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, P, P]
+        L.orc_ref_fix_sinogram.argtypes = [P, P, ctypes.c_int, ctypes.c_int, ctypes.c_double]
+        L.orc_ref_window.restype = ctypes.c_float
+        L.orc_ref_window.argtypes = [ctypes.c_int, ctypes.c_uint, ctypes.c_uint]
+        L.orc_ref_preprocess.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                         ctypes.c_float, ctypes.c_int, P]
+        L.orc_ref_filter_rows.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_ref_backproject.argtypes = [P, ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_int, P]
+        L.orc_ref_reconstruct.restype = ctypes.c_int
+        L.orc_ref_reconstruct.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_float,
+                                          ctypes.c_int, P, ctypes.c_int, P, P]
+        L.orc_f64_preprocess.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_int, ctypes.c_int, P]
+        L.orc_f64_backproject.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, ctypes.c_int, P]
+        L.orc_num_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _depth(img: np.ndarray) -> int:
+    return {np.dtype(np.uint8): 8, np.dtype(np.uint16): 16, np.dtype(np.float32): 32}[img.dtype]
+
+
+# ------------------------------------------------------------------ geometry
+def cylinder_radius(W: int, FCD: float) -> int:
+    return int(lib().orc_ref_cylinder_radius(W, FCD))
+
+
+def clamp_bounds(xf, xt, yf, yt, zf, zt):
+    out = np.zeros(6, np.float32)
+    ok = lib().orc_ref_clamp_bounds(xf, xt, yf, yt, zf, zt, _p(out))
+    return tuple(float(v) for v in out) if ok else None
+
+
+def ref_geom(W, H, FCD, uOffset=0.0, rel=(0, 1, 0, 1, 0, 1)) -> OrcGeom:
+    g = OrcGeom()
+    r = np.asarray(rel, np.float32)
+    lib().orc_ref_geom(W, H, FCD, uOffset, _p(r), ctypes.byref(g))
+    return g
+
+
+def custom_geom(W, H, FCD, grid, vs, uOffset=0.0, box=None, radius=None) -> OrcGeom:
+    """Grid of arbitrary size and voxel pitch `vs` (in detector pixels)."""
+    g = OrcGeom()
+    g.W, g.H, g.FCD, g.uOffset = W, H, FCD, uOffset
+    g.radius = float(cylinder_radius(W, FCD) if radius is None else radius)
+    g.xSize, g.ySize, g.zSize = grid
+    if box is None:
+        box = (0, grid[0], 0, grid[1], 0, grid[2])
+    g.xFrom, g.xTo, g.yFrom, g.yTo, g.zFrom, g.zTo = box
+    g.vs = vs
+    return g
+
+
+def fix_sinogram(angles, heights, ccw: bool, pixel_size: float):
+    a = np.array(angles, np.float64)
+    h = np.array(heights, np.float64)
+    lib().orc_ref_fix_sinogram(_p(a), _p(h), len(a), int(bool(ccw)), float(pixel_size))
+    return a, h
+
+
+# --------------------------------------------------------- reference FP32 path
+def window(filter_type: int, k: int, nyq: int) -> float:
+    return float(lib().orc_ref_window(filter_type, k, nyq))
+
+
+def ref_preprocess(img: np.ndarray, base: float, FCD: float, filter_type: int) -> np.ndarray:
+    img = np.ascontiguousarray(img)
+    H, W = img.shape
+    out = np.empty((H, W), np.float32)
+    lib().orc_ref_preprocess(_p(img), _depth(img), W, H, base, FCD, filter_type, _p(out))
+    return out
+
+
+def ref_filter_rows(rows: np.ndarray, filter_type: int) -> np.ndarray:
+    out = np.array(rows, np.float32, copy=True, order="C")
+    H, W = out.shape
+    lib().orc_ref_filter_rows(_p(out), W, H, filter_type)
+    return out
+
+
+def ref_backproject(proj: np.ndarray, angles, heights, g: OrcGeom, step: int = 1,
+                    nthreads: int = 0) -> np.ndarray:
+    """Filtered projections (V, H, W) float32 -> Z_FASTEST volume (x, y, z)."""
+    proj = np.ascontiguousarray(proj, np.float32)
+    a = np.ascontiguousarray(angles, np.float64)
+    h = np.ascontiguousarray(heights, np.float64)
+    vol = np.zeros(g.box, np.float32)
+    lib().orc_ref_backproject(_p(proj), proj.shape[0], step, _p(a), _p(h), ctypes.byref(g), nthreads, _p(vol))
+    return vol
+
+
+def ref_reconstruct(imgs: np.ndarray, angles, heights, base: float, filter_type: int, g: OrcGeom,
+                    step: int = 1, nthreads: int = 0):
+    """Whole reference CPU path from raw images (V, H, W). Returns (volume x,y,z, seconds)."""
+    imgs = np.ascontiguousarray(imgs)
+    a = np.ascontiguousarray(angles, np.float64)
+    h = np.ascontiguousarray(heights, np.float64)
+    vol = np.zeros(g.box, np.float32)
+    secs = ctypes.c_double(0)
+    lib().orc_ref_reconstruct(_p(imgs), _depth(imgs[0]), imgs.shape[0], step, _p(a), _p(h), base,
+                              filter_type, ctypes.byref(g), nthreads, _p(vol), ctypes.byref(secs))
+    return vol, secs.value
+
+
+# ----------------------------------------------------------------- FP64 oracle
+def f64_preprocess(img: np.ndarray, base: float, FCD: float, filter_type: int, pad: int = 1) -> np.ndarray:
+    img = np.ascontiguousarray(img)
+    H, W = img.shape
+    out = np.empty((H, W), np.float64)
+    lib().orc_f64_preprocess(_p(img), _depth(img), W, H, base, FCD, filter_type, pad, _p(out))
+    return out
+
+
+def f64_backproject(proj: np.ndarray, angles, heights, g: OrcGeom, z0: int = 0, z1: int = 0) -> np.ndarray:
+    proj = np.ascontiguousarray(proj, np.float64)
+    a = np.ascontiguousarray(angles, np.float64)
+    h = np.ascontiguousarray(heights, np.float64)
+    bx, by, bz = g.box
+    nz = (z1 - z0) if z1 > z0 else bz
+    vol = np.zeros((bx, by, nz), np.float64)
+    lib().orc_f64_backproject(_p(proj), proj.shape[0], _p(a), _p(h), ctypes.byref(g), z0, z1, _p(vol))
+    return vol
+
+
+def f64_reconstruct(imgs, angles, heights, base, filter_type, g: OrcGeom, pad=1, z0=0, z1=0):
+    proj = np.stack([f64_preprocess(im, base, g.FCD, filter_type, pad) for im in imgs])
+    return f64_backproject(proj, angles, heights, g, z0, z1)
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())
+
+
+@dataclass
+class RelErr:
+    rel_l2: float
+    max_abs: float
+
+
+def rel_err(x: np.ndarray, ref: np.ndarray) -> RelErr:
+    x = np.asarray(x, np.float64)
+    ref = np.asarray(ref, np.float64)
+    d = x - ref
+    n = np.linalg.norm(ref.ravel())
+    return RelErr(float(np.linalg.norm(d.ravel()) / (n if n > 0 else 1.0)), float(np.abs(d).max(initial=0.0)))

@@ -1,0 +1,149 @@
+"""C ABI checks that need no GPU: the library loads, exports every function
+include/ctb.h declares, and the host-side logic (CSV ingest, image decoding,
+grid rule, bounds) follows the reference."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import ct_b200
+from ct_b200 import CtbError, CtVolume, synth
+from ct_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "ctb.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(ctb_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(L.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python binding declares a signature for each of them
+    assert set(names) <= set(L.SIGNATURES), set(names) - set(L.SIGNATURES)
+
+
+def test_reference_grid_matches_oracle(oracle):
+    from ct_b200 import ops
+    for W, H, D in [(256, 192, 1000.0), (1024, 1024, 2500.0), (2048, 2048, 5000.0), (300, 77, 301.5)]:
+        d, g = ops.detector(W, H, D)
+        og = oracle.ref_geom(W, H, D)
+        assert (g.x_size, g.y_size, g.z_size) == (og.xSize, og.ySize, og.zSize)
+        assert d.radius == og.radius
+    d, g = ops.detector(256, 192, 1000.0, rel=(0.25, 0.75, 0.1, 0.3, 0.0, 0.2))
+    og = oracle.ref_geom(256, 192, 1000.0, rel=oracle.clamp_bounds(0.25, 0.75, 0.1, 0.3, 0.0, 0.2))
+    assert (g.x_from, g.x_to, g.y_from, g.y_to, g.z_from, g.z_to) == (
+        og.xFrom, og.xTo, og.yFrom, og.yTo, og.zFrom, og.zTo)
+
+
+def write_scan(tmp_path, V=6, H=8, W=12, rotation="ccw", heights=None, angles=None):
+    geom = synth.ScanGeometry(V, W, H, pitch_mm=1.0, sod_mm=100.0, sdd_mm=200.0)
+    imgs = np.random.default_rng(0).integers(1000, 60000, (V, H, W)).astype(np.uint16)
+    csv = synth.write_scan(str(tmp_path), imgs, geom, rotation=rotation, heights_mm=heights, angles_deg=angles)
+    return csv, imgs, geom
+
+
+def test_csv_ingest_geometry(tmp_path, oracle):
+    csv, imgs, geom = write_scan(tmp_path, heights=[0.0, 0.5, 1.0, 1.5, 2.0, 2.5])
+    v = CtVolume(csv)
+    assert v.getSinogramSize() == 6
+    assert (v.getImageWidth(), v.getImageHeight()) == (12, 8)
+    # FCD / pixelSize in float (Ct/CtVolume.cpp:170)
+    assert v.getFCD() == np.float32(100.0) / np.float32(0.5)
+    assert v.getPixelSize() == pytest.approx(0.5)
+    og = oracle.ref_geom(12, 8, float(np.float32(100.0) / np.float32(0.5)))
+    assert (v.getXSize(), v.getYSize(), v.getZSize()) == (og.xSize, og.ySize, og.zSize)
+    v.setVolumeBounds(0.25, 0.75, 0.0, 1.0, 0.5, 1.0)
+    g = v.grid()
+    assert (g.x_from, g.x_to, g.z_from, g.z_to) == (int(0.25 * og.xSize + 0.5), int(0.75 * og.xSize + 0.5), 4, 8)
+
+
+def test_csv_tiff_and_png_decoding(tmp_path):
+    """Same pixels through PGM, TIFF (II and MM) and PNG give the same detector data."""
+    import zlib, struct
+    from ct_b200 import ops  # noqa: F401
+    H, W = 5, 7
+    img = np.arange(H * W, dtype=np.uint16).reshape(H, W) * 997
+    d = tmp_path / "imgs"
+    d.mkdir()
+
+    def tiff(path, a, be):
+        e = ">" if be else "<"
+        data = a.astype(e + "u2").tobytes()
+        ntags = 8
+        ifd_off = 8
+        data_off = ifd_off + 2 + ntags * 12 + 4
+        tags = [(256, 3, 1, W), (257, 3, 1, H), (258, 3, 1, 16), (259, 3, 1, 1), (262, 3, 1, 1),
+                (273, 4, 1, data_off), (278, 3, 1, H), (279, 4, 1, len(data))]
+        out = (b"MM" if be else b"II") + struct.pack(e + "HI", 42, ifd_off) + struct.pack(e + "H", ntags)
+        for tag, typ, cnt, val in tags:
+            if typ == 3:
+                out += struct.pack(e + "HHIHH", tag, typ, cnt, val, 0)
+            else:
+                out += struct.pack(e + "HHII", tag, typ, cnt, val)
+        out += struct.pack(e + "I", 0) + data
+        open(path, "wb").write(out)
+
+    def png(path, a):
+        raw = b"".join(b"\x00" + row.astype(">u2").tobytes() for row in a)
+        def chunk(t, b):
+            return struct.pack(">I", len(b)) + t + b + struct.pack(">I", zlib.crc32(t + b) & 0xffffffff)
+        ihdr = struct.pack(">IIBBBBB", W, H, 16, 0, 0, 0, 0)
+        open(path, "wb").write(b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", ihdr) + chunk(b"IDAT", zlib.compress(raw)) +
+                               chunk(b"IEND", b""))
+
+    synth.write_pgm16(str(d / "a.pgm"), img)
+    tiff(str(d / "b.tif"), img, False)
+    tiff(str(d / "c.tif"), img, True)
+    png(str(d / "d.png"), img)
+    csv = tmp_path / "s.csv"
+    csv.write_text("imgs\n0.5\nccw\n0\n100\n1\nx\na.pgm\t0\nb.tif\t90\nc.tif\t180\nd.png\t270\n")
+    v = CtVolume(str(csv))
+    assert v.getSinogramSize() == 4
+
+
+@pytest.mark.parametrize("body,needle", [
+    ("imgs\nabc\nccw\n0\n100\n1\nx\na.pgm\t0\n", "Could not read the parameters"),
+    ("imgs\n0.5\nccw\n0\n100\n0\nx\na.pgm\t0\n", "base intensity"),
+    ("imgs\n0.5\nccw\n0\n100\n1\nx\n", "does not contain any images"),
+    ("imgs\n0.5\nccw\n0\n100\n1\nx\na.pgm\tzero\n", "image parameters"),
+    ("imgs\n0.5\nccw\n0\n100\n1\nx\nmissing.pgm\t0\n", "Error loading the image"),
+    ("imgs\n0.5\nccw\n0\n3\n1\nx\na.pgm\t0\n", "FCD must be greater than the image width"),
+    ("imgs\n0.5\nccw\n0\n100\n1\nx\na.pgm\t0\nsmall.pgm\t1\n", "dimensions differ"),
+])
+def test_csv_error_branches(tmp_path, body, needle):
+    d = tmp_path / "imgs"
+    d.mkdir()
+    synth.write_pgm16(str(d / "a.pgm"), np.full((4, 6), 1000, np.uint16))
+    synth.write_pgm16(str(d / "small.pgm"), np.full((3, 6), 1000, np.uint16))
+    csv = tmp_path / "s.csv"
+    csv.write_text(body)
+    with pytest.raises(CtbError) as e:
+        CtVolume(str(csv))
+    assert needle in e.value.message
+
+
+def test_csv_direction_and_heights(tmp_path):
+    """cw + increasing angles are negated; blank lines repeat the previous image (reference quirk)."""
+    d = tmp_path / "imgs"
+    d.mkdir()
+    synth.write_pgm16(str(d / "a.pgm"), np.full((4, 6), 1000, np.uint16))
+    csv = tmp_path / "s.csv"
+    csv.write_text("imgs\n0.5\ncw\n0\n100\n1\nx\na.pgm\t0\t1\na.pgm\t10\t2\n\na.pgm\t20\n")
+    v = CtVolume(str(csv))
+    assert v.getSinogramSize() == 4
+
+
+def test_missing_library_fails_loudly(monkeypatch):
+    monkeypatch.setattr(L, "_lib", None)
+    monkeypatch.setattr(L, "LIB_PATH", "/nonexistent/libctb.so")
+    with pytest.raises(RuntimeError):
+        L.lib()

@@ -23,6 +23,7 @@
 #include <cuda_fp16.h>
 
 #include "../ctb_internal.h"
+#include "geom.cuh"
 
 namespace ctb {
 
@@ -59,9 +60,9 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ pro
     const int z0 = blockIdx.z * ZC;
     const int tid = threadIdx.y * kBX + threadIdx.x;
 
-    const float xw = (float(x) - g.xPre) * g.vs;
-    const float yw = (float(y) - g.yPre) * g.vs;
-    const bool live = x < g.X && y < g.Y && (xw * xw + yw * yw) < g.r2;
+    const float xw = world_coord(x, g.xPre, g.vs);
+    const float yw = world_coord(y, g.yPre, g.vs);
+    const bool live = x < g.X && y < g.Y && in_cylinder(xw, yw, g.r2);
     // (z - zPre) is exact for every z; rounding happens once, in the product
     // with the voxel pitch, exactly as the forward projector evaluates it.
     const float zr0 = float(z0) - g.zPre;
@@ -79,25 +80,22 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ pro
         const T* pv = proj + (long long)vb * g.view_stride;
         for (int iv = 0; iv < nv; ++iv, pv += g.view_stride) {
             const float4 q = sviews[iv];  // sin, cos, h
-            float t = (-1) * xw * q.x + yw * q.y;
-            t += g.uOff;
-            const float s = xw * q.y + yw * q.x;
-            const float U = g.D / (g.D - s);
-            const float u = t * U;
+            float U, u;
+            column_geom(xw, yw, q.x, q.y, g.D, g.uOff, &U, &u);
             if (!(u >= g.lbU && u <= g.ubU)) continue;
-            const float w = U * U * g.load_scale;
-            const float ui = u + g.uPre;
+            const float w = __fmul_rn(__fmul_rn(U, U), g.load_scale);
+            const float ui = __fadd_rn(u, g.uPre);
             const int u0 = int(ui);
-            const float fu = ui - float(u0);
+            const float fu = __fsub_rn(ui, float(u0));
             const T* col = pv + u0;
 #pragma unroll
             for (int j = 0; j < ZC; ++j) {
-                const float zw = (zr0 + float(j)) * g.vs;
-                const float v = (zw + q.z) * U;
+                const float zw = __fmul_rn(__fadd_rn(zr0, float(j)), g.vs);
+                float v;
+                const float vi = row_coord(zw, q.z, U, g.vPre, &v);
                 if (v >= g.lbV && v <= g.ubV) {
-                    const float vi = (-1) * v + g.vPre;
                     const int v0 = int(vi);
-                    const float fv = vi - float(v0);
+                    const float fv = __fsub_rn(vi, float(v0));
                     const T* r0 = col + (long long)v0 * g.W;
                     const float a = (1.0f - fu) * ld(r0) + fu * ld(r0 + 1);
                     const float b = (1.0f - fu) * ld(r0 + g.W) + fu * ld(r0 + g.W + 1);

@@ -21,6 +21,7 @@
 // rows -> consecutive z) read contiguous memory.
 
 #include "../ctb_internal.h"
+#include "geom.cuh"
 
 namespace ctb {
 
@@ -61,23 +62,20 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
         const int i1 = min(ns - 1, int(ceil(hi)) + 1);
         for (int is = i0; is <= i1; ++is) {
             const int x = x_major ? ip : is, y = x_major ? is : ip;
-            const float xw = (float(x) - g.xPre) * g.vs;
-            const float yw = (float(y) - g.yPre) * g.vs;
-            if (!((xw * xw + yw * yw) < g.r2)) continue;
-            float t = (-1) * xw * sn + yw * cs;
-            t += g.uOff;
-            const float s = xw * cs + yw * sn;
-            const float U = D / (D - s);
-            const float u = t * U;
+            const float xw = world_coord(x, g.xPre, g.vs);
+            const float yw = world_coord(y, g.yPre, g.vs);
+            if (!in_cylinder(xw, yw, g.r2)) continue;
+            float U, u;
+            column_geom(xw, yw, sn, cs, D, g.uOff, &U, &u);
             if (!(u >= g.lbU && u <= g.ubU)) continue;
-            const float ui = u + g.uPre;
+            const float ui = __fadd_rn(u, g.uPre);
             const int u0 = int(ui);
-            const float fu = ui - float(u0);
+            const float fu = __fsub_rn(ui, float(u0));
             float bu;
             if (u0 == c) bu = 1.0f - fu;
             else if (u0 + 1 == c) bu = fu;
             else continue;
-            const float w = U * U * g.load_scale;
+            const float w = __fmul_rn(__fmul_rn(U, U), g.load_scale);
             // rows: vi = vPre - (zw + h) U in [r-1, r+1)  ->  z range
             const float* col = volz + ((long long)x * g.Y + y) * g.Zs;
             const double zlo = ((double(g.vPre) - (r + 1)) / U - h) / g.vs + g.zPre;
@@ -85,12 +83,12 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
             const int z0 = max(0, int(floor(zlo)) - 1);
             const int z1 = min(g.Zs - 1, int(ceil(zhi)) + 1);
             for (int z = z0; z <= z1; ++z) {
-                const float zw = (float(z) - g.zPre) * g.vs;
-                const float v = (zw + h) * U;
+                const float zw = world_coord(z, g.zPre, g.vs);
+                float v;
+                const float vi = row_coord(zw, h, U, g.vPre, &v);
                 if (!(v >= g.lbV && v <= g.ubV)) continue;
-                const float vi = (-1) * v + g.vPre;
                 const int v0 = int(vi);
-                const float fv = vi - float(v0);
+                const float fv = __fsub_rn(vi, float(v0));
                 float bv;
                 if (v0 == r) bv = 1.0f - fv;
                 else if (v0 + 1 == r) bv = fv;

@@ -315,9 +315,10 @@ void backproject_view_ref(const float* image, const orc_geom& g, const RefBounds
 }
 
 // ------------------------------------------------------------- FP64 oracle
-void preprocess_f64(const void* img, int depth, int W, int H, double base, double FCD,
+// Rows [r0, r0 + nrows) of a projection of height H; img points at row r0.
+void preprocess_f64(const void* img, int depth, int W, int H, int r0, int nrows, double base, double FCD,
                     int filter, int pad, double* out) {
-    const size_t n = size_t(W) * H;
+    const size_t n = size_t(W) * nrows;
     std::vector<double> p(n);
     for (size_t i = 0; i < n; ++i) {
         double s;
@@ -328,12 +329,15 @@ void preprocess_f64(const void* img, int depth, int W, int H, double base, doubl
         p[i] = -std::log(s / (base + 0.000001 * base));
     }
     const double uPre = W / 2.0, vPre = H / 2.0;
-    for (int r = 0; r < H; ++r)
+    for (int r = 0; r < nrows; ++r)
         for (int c = 0; c < W; ++c) {
-            const double u = c - uPre, v = -r + vPre;
+            const double u = c - uPre, v = -(r + r0) + vPre;
             p[size_t(r) * W + c] *= FCD / std::sqrt(FCD * FCD + u * u + v * v);
         }
-    const size_t N = size_t(W) * size_t(pad < 1 ? 1 : pad);
+    // pad 1: the reference's length-W circular filter; pad >= 2: zero padding
+    // to the next power of two >= 2W with the window sampled on that grid
+    size_t N = size_t(W);
+    if (pad >= 2) { N = 1; while (N < 2 * size_t(W)) N <<= 1; }
     const size_t nyq = N / 2 + 1;
     const Dft dft(N);
     std::vector<double> win(N);
@@ -341,7 +345,7 @@ void preprocess_f64(const void* img, int depth, int W, int H, double base, doubl
     // output scale follows the reference's x W convention for every padding
     const double scale = double(W) / double(N);
 #pragma omp parallel for
-    for (int r = 0; r < H; ++r) {
+    for (int r = 0; r < nrows; ++r) {
         std::vector<cd> x(N, cd(0, 0));
         for (int c = 0; c < W; ++c) x[c] = cd(p[size_t(r) * W + c], 0.0);
         dft.run(x, false);
@@ -455,17 +459,37 @@ int orc_ref_reconstruct(const void* imgs, int depth, int nviews, int step, const
 
 // ------------------------------------------------------------- FP64 oracle
 // Preprocess one projection in double: log, Feldkamp weight, ramp filter with
-// the transform length N = pad * W (zero padded), window sampled on that grid,
-// output scaled by W/N so every padding keeps the reference's x W convention.
+// the transform length N = W (pad 1) or the next power of two >= 2W (pad 2,
+// zero padded), window sampled on that grid, output scaled by W/N so every
+// padding keeps the reference's x W convention.
 void orc_f64_preprocess(const void* img, int depth, int W, int H, double base, double FCD,
                         int filter, int pad, double* out) {
-    preprocess_f64(img, depth, W, H, base, FCD, filter, pad, out);
+    preprocess_f64(img, depth, W, H, 0, H, base, FCD, filter, pad, out);
+}
+
+// The same for the detector rows [r0, r0 + nrows) only; img points at row r0.
+void orc_f64_preprocess_rows(const void* img, int depth, int W, int H, int r0, int nrows, double base,
+                             double FCD, int filter, int pad, double* out) {
+    preprocess_f64(img, depth, W, H, r0, nrows, base, FCD, filter, pad, out);
 }
 
 // Double-precision voxel-driven backprojection of filtered projections into a
 // Z_FASTEST volume, restricted to z indices [z0, z1) of the box when z1 > z0.
+// Projections hold detector rows [row0, row0 + nrows) of every view; samples
+// outside that window are counted in *missed (the caller sizes the window).
+int orc_f64_backproject_rows(const double* proj, int nviews, const double* anglesDeg,
+                             const double* heightsPx, const orc_geom* g, int row0, int nrows, int z0, int z1,
+                             double* vol, long long* missed);
+
 void orc_f64_backproject(const double* proj, int nviews, const double* anglesDeg,
                          const double* heightsPx, const orc_geom* g, int z0, int z1, double* vol) {
+    long long missed = 0;
+    orc_f64_backproject_rows(proj, nviews, anglesDeg, heightsPx, g, 0, g->H, z0, z1, vol, &missed);
+}
+
+int orc_f64_backproject_rows(const double* proj, int nviews, const double* anglesDeg,
+                             const double* heightsPx, const orc_geom* g, int row0, int nrows, int z0, int z1,
+                             double* vol, long long* missed) {
     const int W = g->W, H = g->H;
     const double uPre = W / 2.0, vPre = H / 2.0;
     const double xPre = g->xSize / 2.0 - g->xFrom, yPre = g->ySize / 2.0 - g->yFrom,
@@ -475,11 +499,12 @@ void orc_f64_backproject(const double* proj, int nviews, const double* anglesDeg
     const int zn = z1 - z0;
     const double lbU = -uPre, ubU = (W - 1.1) - uPre, lbV = -(H - 1.1) + vPre, ubV = vPre;
     const double D = g->FCD, vs = g->vs, r2 = double(g->radius) * g->radius;
+    long long miss = 0;
     for (int p = 0; p < nviews; ++p) {
         const double th = anglesDeg[p] / 180.0 * M_PI, sn = std::sin(th), cs = std::cos(th);
         const double h = heightsPx[p];
-        const double* img = proj + size_t(p) * W * H;
-#pragma omp parallel for schedule(dynamic)
+        const double* img = proj + size_t(p) * W * nrows;
+#pragma omp parallel for schedule(dynamic) reduction(+ : miss)
         for (int xi = 0; xi < xMax; ++xi) {
             const double x = (xi - xPre) * vs;
             for (int yi = 0; yi < yMax; ++yi) {
@@ -498,7 +523,8 @@ void orc_f64_backproject(const double* proj, int nviews, const double* anglesDeg
                     const double vi = -v + vPre;
                     const int v0 = int(vi);
                     const double fv = vi - v0;
-                    const double* r0 = img + size_t(v0) * W;
+                    if (v0 < row0 || v0 + 1 >= row0 + nrows) { ++miss; continue; }
+                    const double* r0 = img + size_t(v0 - row0) * W;
                     const double* r1 = r0 + W;
                     const double a = (1 - fu) * r0[u0] + fu * r0[u0 + 1];
                     const double c = (1 - fu) * r1[u0] + fu * r1[u0 + 1];
@@ -507,6 +533,8 @@ void orc_f64_backproject(const double* proj, int nviews, const double* anglesDeg
             }
         }
     }
+    *missed = miss;
+    return miss == 0 ? 0 : 1;
 }
 
 int orc_num_threads(void) { return omp_get_max_threads(); }

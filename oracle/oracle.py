@@ -71,6 +71,12 @@ def lib():
         L.orc_f64_preprocess.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_int, ctypes.c_int, P]
         L.orc_f64_backproject.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, ctypes.c_int, P]
+        L.orc_f64_preprocess_rows.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                              ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                              ctypes.c_int, P]
+        L.orc_f64_backproject_rows.restype = ctypes.c_int
+        L.orc_f64_backproject_rows.argtypes = [P, ctypes.c_int, P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                               ctypes.c_int, P, P]
         L.orc_num_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -189,6 +195,29 @@ def f64_backproject(proj: np.ndarray, angles, heights, g: OrcGeom, z0: int = 0, 
 def f64_reconstruct(imgs, angles, heights, base, filter_type, g: OrcGeom, pad=1, z0=0, z1=0):
     proj = np.stack([f64_preprocess(im, base, g.FCD, filter_type, pad) for im in imgs])
     return f64_backproject(proj, angles, heights, g, z0, z1)
+
+
+def f64_slices(imgs_rows: np.ndarray, row0: int, H: int, angles, heights, base: float, filter_type: int,
+               g: OrcGeom, z0: int, z1: int, pad: int = 1) -> np.ndarray:
+    """FP64 reconstruction of box slices [z0, z1) from detector rows [row0, row0 + n) of every view
+    (imgs_rows: (V, n, W)). Raises if a sample falls outside the row window."""
+    imgs_rows = np.ascontiguousarray(imgs_rows)
+    V, n, W = imgs_rows.shape
+    proj = np.empty((V, n, W), np.float64)
+    L = lib()
+    for k in range(V):
+        L.orc_f64_preprocess_rows(_p(imgs_rows[k]), _depth(imgs_rows[k]), W, H, row0, n, base, g.FCD,
+                                  filter_type, pad, _p(proj[k]))
+    a = np.ascontiguousarray(angles, np.float64)
+    h = np.ascontiguousarray(heights, np.float64)
+    bx, by, _ = g.box
+    vol = np.zeros((bx, by, z1 - z0), np.float64)
+    missed = ctypes.c_longlong(0)
+    L.orc_f64_backproject_rows(_p(proj), V, _p(a), _p(h), ctypes.byref(g), row0, n, z0, z1, _p(vol),
+                               ctypes.byref(missed))
+    if missed.value:
+        raise ValueError(f"{missed.value} samples outside detector rows [{row0}, {row0 + n})")
+    return vol
 
 
 def num_threads() -> int:

@@ -1,0 +1,321 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bars: FP32 filtering <= 1e-5 relative per projection, FP32 backprojection
+<= 1e-5 relative L2 on identical filtered input, end-to-end FP32 reconstruction
+<= 1e-4 relative L2 against the reference's CPU path restated by the oracle,
+FP16/BF16 storage <= 1e-3 relative L2 against the FP64 oracle.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+import ct_b200  # noqa: E402
+from ct_b200 import CtVolume, ops, synth  # noqa: E402
+from ct_b200 import _lib as L  # noqa: E402
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    torch.cuda.init()
+
+
+def np_phantom_images(V, H, W, FCD_px, pix_mm, n_ell=6, seed=0, photons=None, heights_mm=None, uoff_mm=0.0):
+    from oracle import phantom
+    geom = synth.ScanGeometry(V, W, H, pitch_mm=pix_mm * 2, sod_mm=FCD_px * pix_mm, sdd_mm=FCD_px * pix_mm * 2)
+    r_mm, hz_mm = synth.fov(geom)
+    ell = synth.random_ellipsoids(np.random.default_rng(seed), n_ell, r_mm, hz_mm, axes_mm=(0.1 * r_mm, 0.6 * r_mm))
+    p = phantom.project(ell, geom.angles(), heights_mm, W, H, geom.pixel_eff, geom.sod_mm, uoff_mm)
+    return synth.intensities_from_line_integrals(p, photons, seed), geom, ell
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+# ------------------------------------------------------------------ phantom
+def test_phantom_kernel_matches_numpy():
+    from oracle import phantom
+    rng = np.random.default_rng(1)
+    ell = synth.random_ellipsoids(rng, 5, 10.0, 8.0, axes_mm=(2.0, 8.0))
+    ang = np.array([0.0, 33.0, 190.5])
+    h = np.array([0.3, -0.2, 0.0])
+    ref = phantom.project(ell, ang, h, 20, 16, 0.5, 60.0, 0.7)
+    out = ops.phantom_project(ell, ang, h, 20, 16, 0.5, 60.0, 0.7).cpu().numpy()
+    assert np.abs(out - ref).max() <= 1e-9 * max(1.0, np.abs(ref).max())
+
+
+# ------------------------------------------------------------------ filter
+@pytest.mark.parametrize("W", [16, 17, 64, 100, 255, 256])
+@pytest.mark.parametrize("ft", [0, 1, 2])
+def test_filter_fp32_matches_reference_path(oracle, W, ft):
+    rng = np.random.default_rng(W * 10 + ft)
+    V, H = 3, 7
+    imgs = rng.integers(2000, 65535, size=(V, H, W)).astype(np.uint16)
+    FCD = 4.0 * W
+    det, _ = ops.detector(W, H, FCD)
+    raw = torch.from_numpy(imgs.astype(np.int32)).to(torch.uint16).cuda()
+    out = ops.filter_projections(raw, det, ft, 1, L.FP32).cpu().numpy()
+    for v in range(V):
+        ref = oracle.ref_preprocess(imgs[v], 1.0, FCD, ft)
+        assert rel_l2(out[v], ref) < 1e-5, (v, rel_l2(out[v], ref))
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.float32])
+def test_filter_other_depths(oracle, dtype):
+    rng = np.random.default_rng(5)
+    V, H, W = 2, 6, 48
+    if dtype == np.uint8:
+        imgs = rng.integers(10, 255, size=(V, H, W)).astype(np.uint8)
+        raw = torch.from_numpy(imgs).cuda()
+        base = 0.95
+    else:
+        imgs = rng.uniform(0.05, 1.0, size=(V, H, W)).astype(np.float32)
+        raw = torch.from_numpy(imgs).cuda()
+        base = 1.1
+    det, _ = ops.detector(W, H, 200.0, base_intensity=base)
+    out = ops.filter_projections(raw, det, 1, 1, L.FP32).cpu().numpy()
+    for v in range(V):
+        assert rel_l2(out[v], oracle.ref_preprocess(imgs[v], base, 200.0, 1)) < 1e-5
+
+
+@pytest.mark.parametrize("W", [64, 100])
+def test_filter_padded_matches_fp64_oracle(oracle, W):
+    rng = np.random.default_rng(7)
+    V, H = 2, 5
+    imgs = rng.integers(2000, 65535, size=(V, H, W)).astype(np.uint16)
+    det, _ = ops.detector(W, H, 500.0)
+    raw = torch.from_numpy(imgs.astype(np.int32)).to(torch.uint16).cuda()
+    out = ops.filter_projections(raw, det, 2, 2, L.FP32).cpu().numpy()
+    for v in range(V):
+        assert rel_l2(out[v], oracle.f64_preprocess(imgs[v], 1.0, 500.0, 2, pad=2)) < 1e-5
+
+
+@pytest.mark.parametrize("store", [L.FP16, L.BF16])
+def test_filter_half_storage(oracle, store):
+    rng = np.random.default_rng(9)
+    V, H, W = 2, 8, 128
+    imgs = rng.integers(2000, 65535, size=(V, H, W)).astype(np.uint16)
+    det, _ = ops.detector(W, H, 600.0)
+    raw = torch.from_numpy(imgs.astype(np.int32)).to(torch.uint16).cuda()
+    out = ops.filter_projections(raw, det, 0, 1, store, 1.0 / W).float().cpu().numpy() * W
+    tol = 2e-3 if store == L.FP16 else 1e-2
+    for v in range(V):
+        assert rel_l2(out[v], oracle.f64_preprocess(imgs[v], 1.0, 600.0, 0)) < tol
+
+
+# ----------------------------------------------------------- backprojection
+def filtered_set(oracle, V=40, H=24, W=32, FCD=100.0, ft=0, seed=0):
+    imgs, geom, _ = np_phantom_images(V, H, W, FCD, 0.5, seed=seed)
+    proj = np.stack([oracle.ref_preprocess(im, 1.0, FCD, ft) for im in imgs])
+    return imgs, proj, geom.angles()
+
+
+def gpu_bp(proj, angles, heights, det, grid, z_begin=0, z_end=None, accumulate_into=None):
+    t = torch.from_numpy(proj).cuda()
+    out = None if accumulate_into is None else accumulate_into
+    vol = ops.backproject(t, angles, heights, det, grid, z_begin, z_end, out=out,
+                          accumulate=accumulate_into is not None)
+    torch.cuda.synchronize()
+    return vol.cpu().numpy()  # (Zs, Y, X)
+
+
+def test_backproject_fp32_matches_reference_path(oracle):
+    imgs, proj, ang = filtered_set(oracle)
+    V, H, W = proj.shape
+    det, grid = ops.detector(W, H, 100.0)
+    og = oracle.ref_geom(W, H, 100.0)
+    ref = oracle.ref_backproject(proj, ang, np.zeros(V), og)  # (x, y, z)
+    out = gpu_bp(proj, ang, None, det, grid)
+    assert rel_l2(out.transpose(2, 1, 0), ref) < 1e-5
+
+
+def test_backproject_subbox_offsets_slabs(oracle):
+    imgs, proj, ang = filtered_set(oracle, V=30, H=20, W=28, FCD=90.0, ft=2, seed=3)
+    V, H, W = proj.shape
+    rel = (0.2, 0.8, 0.1, 0.7, 0.25, 0.9)
+    det, grid = ops.detector(W, H, 90.0, u_offset=1.25, rel=rel)
+    og = oracle.ref_geom(W, H, 90.0, 1.25, rel=oracle.clamp_bounds(*rel))
+    heights = np.linspace(-1.5, 1.5, V)
+    ref = oracle.ref_backproject(proj, ang, heights, og)
+    X, Y, Z = grid.box
+    # three uneven slabs into one buffer
+    vol = torch.zeros((Z, Y, X), device="cuda")
+    cuts = [0, 3, 9, Z]
+    for a, b in zip(cuts[:-1], cuts[1:]):
+        ops.backproject(torch.from_numpy(proj).cuda(), ang, heights, det, grid, a, b, out=vol[a:b])
+    out = vol.cpu().numpy()
+    assert rel_l2(out.transpose(2, 1, 0), ref) < 1e-5
+    # accumulate: two halves of the views add up to the whole
+    half = V // 2
+    acc = torch.zeros((Z, Y, X), device="cuda")
+    pt = torch.from_numpy(proj).cuda()
+    ops.backproject(pt[:half].contiguous(), ang[:half], heights[:half], det, grid, out=acc, accumulate=True)
+    ops.backproject(pt[half:].contiguous(), ang[half:], heights[half:], det, grid, out=acc, accumulate=True)
+    assert rel_l2(acc.cpu().numpy().transpose(2, 1, 0), ref) < 1e-5
+
+
+def test_backproject_binned_grid(oracle):
+    """Voxel pitch 2 detector pixels and a z extent beyond the detector (grid extension)."""
+    imgs, proj, ang = filtered_set(oracle, V=24, H=16, W=40, FCD=150.0, seed=4)
+    V, H, W = proj.shape
+    det, _ = ops.detector(W, H, 150.0)
+    grid = ops.custom_grid(det, (20, 22, 12), 2.0)
+    og = oracle.custom_geom(W, H, 150.0, (20, 22, 12), 2.0)
+    ref = oracle.ref_backproject(proj, ang, np.zeros(V), og)
+    out = gpu_bp(proj, ang, None, det, grid)
+    assert rel_l2(out.transpose(2, 1, 0), ref) < 1e-5
+
+
+# ---------------------------------------------------------------- end to end
+def c1_scan(tmp_path, n_views=360, W=256, H=192, seed=11):
+    """C1: 360 views over 360 deg, 256x192 at 1.0 mm pitch, SOD 500, SDD 1000, 10 ellipsoids."""
+    geom = synth.ScanGeometry(n_views, W, H, pitch_mm=1.0, sod_mm=500.0, sdd_mm=1000.0)
+    scan = synth.make_scan(geom, 10, seed)
+    imgs = scan.images.cpu().numpy()
+    csv = synth.write_scan(str(tmp_path), imgs, geom)
+    return csv, imgs, geom
+
+
+def test_c1_end_to_end_matches_reference_path(oracle, tmp_path):
+    csv, imgs, geom = c1_scan(tmp_path)
+    v = CtVolume(csv)
+    assert (v.getXSize(), v.getYSize(), v.getZSize()) == (252, 252, 192)
+    v.reconstructVolume()
+    out = v.volume(L.Z_FASTEST)
+    og = oracle.ref_geom(geom.width, geom.height, v.getFCD())
+    ref, secs = oracle.ref_reconstruct(imgs, geom.angles(), np.zeros(geom.n_views), 1.0, oracle.RAMLAK, og)
+    err = rel_l2(out, ref)
+    print(f"C1 rel-L2 vs reference CPU path: {err:.3e} (CPU {secs:.2f} s)")
+    assert err <= 1e-4
+
+
+def test_save_formats(oracle, tmp_path):
+    csv, imgs, geom = c1_scan(tmp_path, n_views=24, W=64, H=40)
+    v = CtVolume(csv)
+    v.setVolumeBounds(0.1, 0.9, 0.2, 0.8, 0.0, 0.5)
+    v.setFrequencyFilterType("shepplogan")
+    v.reconstructVolume()
+    X, Y, Z = v.grid().box
+    zf = v.volume(L.Z_FASTEST)
+    for order, endian in [(L.Z_FASTEST, L.LITTLE_ENDIAN), (L.X_FASTEST, L.BIG_ENDIAN),
+                          (L.Z_FASTEST, L.BIG_ENDIAN), (L.X_FASTEST, L.LITTLE_ENDIAN)]:
+        path = tmp_path / f"vol_{order}_{endian}.raw"
+        v.saveVolumeToBinaryFile(str(path), order, endian)
+        data = np.fromfile(path, dtype=">f4" if endian == L.BIG_ENDIAN else "<f4")
+        expect = zf.ravel() if order == L.Z_FASTEST else zf.transpose(2, 1, 0).ravel()
+        assert np.array_equal(data.astype(np.float32), expect)
+        info = (tmp_path / f"vol_{order}_{endian}.txt").read_text()
+        assert f"X size:\t\t\t\t{X}\n" in info and "32bit IEEE 754 float" in info
+        assert ("Z fastest" if order == L.Z_FASTEST else "X fastest") in info
+        vgi = (tmp_path / f"vol_{order}_{endian}.vgi").read_text()
+        assert f"size = {X} {Y} {Z}" in vgi and f"Name = ./vol_{order}_{endian}.raw" in vgi
+    # reconstructInto gives the same bytes as the kept volume, both orders
+    buf = np.empty(X * Y * Z, np.float32)
+    v.reconstructInto(buf.ctypes.data, L.Z_FASTEST)
+    assert np.array_equal(buf, zf.ravel())
+    v.reconstructInto(buf.ctypes.data, L.X_FASTEST)
+    assert np.array_equal(buf, zf.transpose(2, 1, 0).ravel())
+
+
+def test_skip_projections_and_progress(oracle, tmp_path):
+    csv, imgs, geom = c1_scan(tmp_path, n_views=30, W=48, H=32)
+    v = CtVolume(csv)
+    seen = []
+    v.setProgressCallback(lambda s, p: seen.append((s, p)))
+    v.setSkipProjections(2)
+    v.setSlabHeight(16)
+    v.reconstructVolume()
+    out = v.volume(L.Z_FASTEST)
+    og = oracle.ref_geom(48, 32, v.getFCD())
+    ref, _ = oracle.ref_reconstruct(imgs, geom.angles(), np.zeros(30), 1.0, 0, og, step=3)
+    assert rel_l2(out, ref) <= 1e-4
+    assert seen and seen[-1] == (1, 100.0)
+
+
+@pytest.mark.parametrize("store", ["fp16", "bf16"])
+def test_mixed_precision_vs_fp64_oracle(oracle, tmp_path, store):
+    csv, imgs, geom = c1_scan(tmp_path, n_views=120, W=128, H=96, seed=5)
+    v = CtVolume(csv)
+    v.setFrequencyFilterType("hann")
+    v.setPrecision(store)
+    v.reconstructVolume()
+    out = v.volume(L.Z_FASTEST)
+    og = oracle.ref_geom(128, 96, v.getFCD())
+    ref = oracle.f64_reconstruct(imgs, geom.angles(), np.zeros(120), 1.0, oracle.HANN, og)
+    err = rel_l2(out, ref)
+    print(f"{store} rel-L2 vs FP64 oracle: {err:.3e}")
+    assert err <= 1e-3
+
+
+# ------------------------------------------------------------ adjoint pair
+def adjoint_case(V=36, H=20, W=30, grid_size=None, vs=1.0, rel=None, uoff=0.0, heights=False, seed=0):
+    rng = np.random.default_rng(seed)
+    det, grid = ops.detector(W, H, 120.0, u_offset=uoff, rel=rel)
+    if grid_size is not None:
+        grid = ops.custom_grid(det, grid_size, vs)
+    ang = np.sort(rng.uniform(0, 360, V))
+    h = rng.uniform(-2, 2, V) if heights else np.zeros(V)
+    X, Y, Z = grid.box
+    x = torch.from_numpy(rng.standard_normal((Z, Y, X)).astype(np.float32)).cuda()
+    y = torch.from_numpy(rng.standard_normal((V, H, W)).astype(np.float32)).cuda()
+    return det, grid, ang, h, x, y
+
+
+@pytest.mark.parametrize("case", [
+    dict(),
+    dict(rel=(0.1, 0.9, 0.2, 0.7, 0.3, 1.0), uoff=0.8, heights=True),
+    dict(grid_size=(14, 16, 18), vs=2.0),
+    dict(grid_size=(25, 21, 9), vs=1.3, heights=True),
+    dict(V=50, H=33, W=47, seed=2),
+])
+def test_dot_product_adjoint(case):
+    det, grid, ang, h, x, y = adjoint_case(**case)
+    Ax = ops.forward_project(x, ang, h, det, grid)
+    Aty = ops.backproject(y, ang, h, det, grid)
+    torch.cuda.synchronize()
+    lhs = float((Ax.double() * y.double()).sum())
+    rhs = float((x.double() * Aty.double()).sum())
+    assert abs(lhs - rhs) <= 1e-5 * max(abs(lhs), abs(rhs)), (lhs, rhs)
+
+
+def test_forward_slabs_accumulate():
+    det, grid, ang, h, x, y = adjoint_case(heights=True)
+    full = ops.forward_project(x, ang, h, det, grid)
+    Z = grid.box[2]
+    acc = torch.zeros_like(full)
+    for a, b in [(0, 5), (5, 11), (11, Z)]:
+        ops.forward_project(x[a:b].contiguous(), ang, h, det, grid, a, b, out=acc, accumulate=True)
+    torch.cuda.synchronize()
+    assert torch.allclose(acc, full, rtol=1e-5, atol=1e-5)
+
+
+def test_gradient_finite_differences():
+    """grad ||Ax - p||^2 = 2 A^T (Ax - p), checked on 64 random voxels by central differences."""
+    det, grid, ang, h, x, p = adjoint_case(V=30, H=18, W=26, seed=4)
+    rng = np.random.default_rng(8)
+    r = ops.forward_project(x, ang, h, det, grid) - p
+    g = 2.0 * ops.backproject(r.contiguous(), ang, h, det, grid)
+    Z, Y, X = x.shape
+    idx = [(int(rng.integers(Z)), int(rng.integers(Y)), int(rng.integers(X))) for _ in range(64)]
+    base = ops.forward_project(x, ang, h, det, grid).double()
+    eps = 0.5
+    for (k, j, i) in idx:
+        xp = x.clone(); xp[k, j, i] += eps
+        xm = x.clone(); xm[k, j, i] -= eps
+        fp = ops.forward_project(xp, ang, h, det, grid).double() - p.double()
+        fm = ops.forward_project(xm, ang, h, det, grid).double() - p.double()
+        fd = float(((fp * fp) - (fm * fm)).sum()) / (2 * eps)
+        gi = float(g[k, j, i])
+        assert abs(fd - gi) <= 1e-4 * max(1.0, abs(fd)), ((k, j, i), fd, gi)
+    del base

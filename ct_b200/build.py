@@ -30,6 +30,7 @@ CU_FLAGS = ARCH + COMMON + ["--expt-relaxed-constexpr", "-Xptxas", "-warn-spills
 SOURCES = [
     "kernels/filter.cu",
     "kernels/backproject.cu",
+    "kernels/backproject_tma.cu",
     "kernels/forward.cu",
     "kernels/layout.cu",
     "kernels/phantom.cu",
@@ -39,7 +40,7 @@ SOURCES = [
     "host/volume_io.cpp",
     "capi.cpp",
 ]
-HEADERS = ["ctb_internal.h", "host/reconstructor.h", "host/image_io.h"]
+HEADERS = ["ctb_internal.h", "host/reconstructor.h", "host/image_io.h", "kernels/geom.cuh"]
 
 
 def _obj(src: str) -> str:

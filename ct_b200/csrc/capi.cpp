@@ -177,7 +177,10 @@ int ctb_backproject(const void* filtered, int store_type, int n_views, const dou
     int st = upload_views(angles_deg, height_offsets_px, n_views, s, &views);
     if (st != CTB_OK) return st;
     const ctb::ProjGeom g = ctb::proj_geom(*det, *grid, z_begin, z_end, load_scale);
-    st = ctb::backproject_launch(filtered, store_type, views, n_views, g, vol, accumulate, s);
+    double hmax = 0;
+    if (height_offsets_px)
+        for (int i = 0; i < n_views; ++i) hmax = std::max(hmax, std::fabs(height_offsets_px[i]));
+    st = ctb::backproject_launch(filtered, store_type, views, n_views, g, hmax, vol, accumulate, s);
     cudaFreeAsync(views, s);
     return st;
 }

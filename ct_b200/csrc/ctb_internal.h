@@ -82,8 +82,18 @@ struct ProjGeom {
 ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_end, float load_scale);
 
 // Backprojection of views [0, n) from `views` (device view table) into vol.
+// hmax bounds |height offset| (pixels) over the views. Dispatches to the
+// shared-memory (TMA) kernel when possible, else to the global-gather kernel.
 int backproject_launch(const void* proj, int store_type, const float4* views, int n_views,
-                       const ProjGeom& g, float* vol, int accumulate, cudaStream_t s);
+                       const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s);
+int backproject_global_launch(const void* proj, int store_type, const float4* views, int n_views,
+                              const ProjGeom& g, float* vol, int accumulate, cudaStream_t s);
+// Returns CTB_ERR_UNSUPPORTED (nothing launched) when the geometry or layout
+// does not suit the TMA kernel.
+int backproject_tma_launch(const void* proj, int store_type, const float4* views, int n_views,
+                           const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s);
+// Number of CTAs whose bounded mbarrier waits gave up since the last reset.
+int device_wait_timeouts(unsigned* count, int reset);
 
 int forward_launch(const float* vol, const float4* views, int n_views, const ProjGeom& g, float* proj,
                    int accumulate, cudaStream_t s);

@@ -464,7 +464,12 @@ int Reconstructor::run_pipeline(float* out, int order) {
     for (int p = 0; p < int(angles_.size()); p += std::max(1, step_)) used.push_back(p);
     const int V = int(used.size());
     std::vector<double> ang(V), hp(V);
-    for (int i = 0; i < V; ++i) { ang[i] = angles_[used[i]]; hp[i] = heights_px_[used[i]]; }
+    double hmax = 0;
+    for (int i = 0; i < V; ++i) {
+        ang[i] = angles_[used[i]];
+        hp[i] = heights_px_[used[i]];
+        hmax = std::max(hmax, std::fabs(hp[i]));
+    }
 
     const int M = filter_transform_length(W, pad_);
     if (M == 0) return fail(CTB_ERR_UNSUPPORTED, "Detector width exceeds the largest supported FFT length.");
@@ -619,7 +624,7 @@ int Reconstructor::run_pipeline(float* out, int order) {
         if (k >= 2) cudaStreamWaitEvent(s_comp_, ev_down[b], 0);
         const ProjGeom g = proj_geom(det_, grid_, zb, ze, load_scale);
         cudaEventRecord(tb[2 * k], s_comp_);
-        if (backproject_launch(d_filtered_.p, store_, (const float4*)d_views_.p, V, g, (float*)d_slab_[b].p, 0,
+        if (backproject_launch(d_filtered_.p, store_, (const float4*)d_views_.p, V, g, hmax, (float*)d_slab_[b].p, 0,
                                s_comp_))
             return cuda_fail("backprojection launch");
         cudaEventRecord(tb[2 * k + 1], s_comp_);

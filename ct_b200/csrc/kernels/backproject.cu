@@ -20,6 +20,8 @@
 // 128-byte segment of the X-fastest slab.
 
 #include <cuda_bf16.h>
+#include <cstdlib>
+#include <cstring>
 #include <cuda_fp16.h>
 
 #include "../ctb_internal.h"
@@ -169,7 +171,26 @@ ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, i
 }
 
 int backproject_launch(const void* proj, int store_type, const float4* views, int n_views,
-                       const ProjGeom& g, float* vol, int accumulate, cudaStream_t s) {
+                       const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s) {
+    // shared-memory staged kernel when the footprint bound and the 16-byte TMA
+    // stride rule allow it; the global-gather kernel otherwise.
+    // CTB_BP_VARIANT=global|tma forces one of them (tma fails when ineligible).
+    static const int variant = [] {
+        const char* e = std::getenv("CTB_BP_VARIANT");
+        if (!e) return 0;
+        if (!std::strcmp(e, "global")) return 1;
+        if (!std::strcmp(e, "tma")) return 2;
+        return 0;
+    }();
+    if (variant != 1) {
+        const int st = backproject_tma_launch(proj, store_type, views, n_views, g, hmax, vol, accumulate, s);
+        if (st != CTB_ERR_UNSUPPORTED || variant == 2) return st;
+    }
+    return backproject_global_launch(proj, store_type, views, n_views, g, vol, accumulate, s);
+}
+
+int backproject_global_launch(const void* proj, int store_type, const float4* views, int n_views,
+                              const ProjGeom& g, float* vol, int accumulate, cudaStream_t s) {
     switch (store_type) {
         case CTB_FP32: return bp_launch_typed((const float*)proj, views, n_views, g, vol, accumulate, s);
         case CTB_FP16: return bp_launch_typed((const __half*)proj, views, n_views, g, vol, accumulate, s);

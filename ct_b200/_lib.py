@@ -55,6 +55,7 @@ SIGNATURES = {
     "ctb_reference_grid": (I, [P, P, P]),
     "ctb_filter_projections": (I, [P, I, I, P, I, I, P, I, F, P]),
     "ctb_backproject": (I, [P, I, I, P, P, P, P, I, I, F, P, I, P]),
+    "ctb_backproject_noalloc": (I, [P, I, I, P, P, P, P, I, I, F, P, I, P]),
     "ctb_forward_project": (I, [P, P, P, I, P, P, I, I, P, I, P]),
     "ctb_convert_layout": (I, [P, I, I, I, I, I, P, P]),
     "ctb_create": (I, [P]),

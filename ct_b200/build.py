@@ -39,6 +39,7 @@ SOURCES = [
     "host/reconstructor.cpp",
     "host/volume_io.cpp",
     "capi.cpp",
+    "noalloc.cu",
 ]
 HEADERS = ["ctb_internal.h", "host/reconstructor.h", "host/image_io.h", "kernels/geom.cuh"]
 

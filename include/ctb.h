@@ -128,6 +128,20 @@ int ctb_backproject(const void* filtered, int store_type, int n_views, const dou
                     const double* height_offsets_px, const ctb_detector* det, const ctb_grid* grid,
                     int z_begin, int z_end, float load_scale, float* vol, int accumulate, void* stream);
 
+/* ctb_backproject for callers that cannot allocate device memory. No
+ * counterpart in the reference. Same arguments and result as ctb_backproject,
+ * but the per-view geometry table that ctb_backproject allocates on the stream
+ * at every call lives in a static 256 KB device array of the library instead,
+ * so this call allocates nothing (the caller passes the filtered projections
+ * and the volume, as before). At most CTB_NOALLOC_MAX_VIEWS views per call
+ * (CTB_ERR_UNSUPPORTED beyond that). The first call on a device looks up the
+ * array's address; make it before any stream capture. All calls share the
+ * array: calls that overlap on the GPU race, so serialise them. */
+#define CTB_NOALLOC_MAX_VIEWS 8192
+int ctb_backproject_noalloc(const void* filtered, int store_type, int n_views, const double* angles_deg,
+                            const double* height_offsets_px, const ctb_detector* det, const ctb_grid* grid,
+                            int z_begin, int z_end, float load_scale, float* vol, int accumulate, void* stream);
+
 /* Matched forward projector: the exact transpose of ctb_backproject with
  * load_scale = 1 (same bilinear footprint, U^2 weight, cylinder and bounds
  * masks). Input slab as ctb_backproject's output; output n_views x H x W FP32

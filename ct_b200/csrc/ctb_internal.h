@@ -75,6 +75,10 @@ struct ProjGeom {
     float vs;
     float D, uOff, r2;
     float lbU, ubU, lbV, ubV, uPre, vPre;
+    int z_begin;                // first box z index of the slab
+    float zpv;                  // zPre(box) * vs: row lines use box z indices, so a
+                                // voxel's row coordinate does not depend on the slabbing
+    float vi_hi;                // largest valid row coordinate: float(H - 1.1)
     float load_scale;
     long long view_stride;      // elements between consecutive projections
 };

@@ -65,9 +65,6 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ pro
     const float xw = world_coord(x, g.xPre, g.vs);
     const float yw = world_coord(y, g.yPre, g.vs);
     const bool live = x < g.X && y < g.Y && in_cylinder(xw, yw, g.r2);
-    // (z - zPre) is exact for every z; rounding happens once, in the product
-    // with the voxel pitch, exactly as the forward projector evaluates it.
-    const float zr0 = float(z0) - g.zPre;
 
     float acc[ZC];
 #pragma unroll
@@ -90,12 +87,11 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ pro
             const int u0 = int(ui);
             const float fu = __fsub_rn(ui, float(u0));
             const T* col = pv + u0;
+            const RowLine rl = row_line(U, q.z, g.zpv, g.vs, g.vPre);
 #pragma unroll
             for (int j = 0; j < ZC; ++j) {
-                const float zw = __fmul_rn(__fadd_rn(zr0, float(j)), g.vs);
-                float v;
-                const float vi = row_coord(zw, q.z, U, g.vPre, &v);
-                if (v >= g.lbV && v <= g.ubV) {
+                const float vi = row_at(rl, float(g.z_begin + z0 + j));
+                if (row_ok(vi, g.vi_hi)) {
                     const int v0 = int(vi);
                     const float fv = __fsub_rn(vi, float(v0));
                     const T* r0 = col + (long long)v0 * g.W;
@@ -142,6 +138,8 @@ int view_table_build(const double* angles_deg_dev, const double* heights_dev, in
     return cuda_status(cudaGetLastError(), "view_table_kernel launch");
 }
 
+static inline float __fmul_rn_host(float a, float b) { return a * b; }
+
 ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_end, float load_scale) {
     ProjGeom g;
     g.W = det.width;
@@ -165,6 +163,9 @@ ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, i
     g.ubU = float(double(det.width) - 1 - 0.1) - g.uPre;
     g.lbV = (-1) * float(double(det.height) - 1 - 0.1) + g.vPre;
     g.ubV = (-1) * 0.0f + g.vPre;
+    g.z_begin = z_begin;
+    g.zpv = __fmul_rn_host(zPre, g.vs);
+    g.vi_hi = float(double(det.height) - 1 - 0.1);
     g.load_scale = load_scale;
     g.view_stride = (long long)det.width * det.height;
     return g;

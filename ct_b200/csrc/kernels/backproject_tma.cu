@@ -4,8 +4,8 @@
 // from shared memory instead of through L1 gathers.
 //
 // Tile: 32 (x) x 8 (y) columns x ZC (z) voxels per CTA, one column of ZC
-// voxels per thread (sums in registers across all views, as in the global
-// variant). For every view, warp 0 projects the 4 (x, y) corners of the tile
+// voxels per consumer thread (sums in registers across all views, as in the
+// global variant). For every view, a producer warp projects the 4 (x, y) corners of the tile
 // at the two z extremes with the same arithmetic as the voxels (u is a
 // linear-fractional function of (x, y), v is monotone in z and U, so the
 // extremes sit at the corners), rounds the box origin down to a 16-byte
@@ -35,7 +35,7 @@ __device__ unsigned int g_wait_timeouts = 0;
 
 namespace {
 
-constexpr int kTX = 32, kTY = 8, kNBuf = 3;
+constexpr int kTX = 32, kTY = 8;
 constexpr unsigned kWaitLimit = 1u << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -90,104 +90,158 @@ struct Box {
     float vi_hi;         // upper bound of the row coordinate: float(H - 1.1)
 };
 
-template <typename T, int ZC>
-__global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
-                                                           const T* __restrict__ proj,
-                                                           const float4* __restrict__ views, int n_views,
-                                                           ProjGeom g, Box bx, float* __restrict__ vol,
-                                                           int accumulate) {
+// 8 consumer warps own the tile's columns; warp 8 is the producer that waits
+// for a free buffer, projects the tile corners and issues the box load, so
+// box loads run ahead of the compute independently of any consumer warp.
+constexpr int kConsumerWarps = kTX * kTY / 32;
+constexpr int kThreads = (kConsumerWarps + 1) * 32;
+
+template <typename T, int ZC, int NBUF>
+__global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+                                                          const T* __restrict__ proj,
+                                                          const float4* __restrict__ views, int n_views,
+                                                          ProjGeom g, Box bx, float* __restrict__ vol,
+                                                          int accumulate) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t mbar[kNBuf];
-    __shared__ int2 org[kNBuf];
-    __shared__ int ovf[kNBuf];
-    __shared__ int abort_flag;
+    __shared__ __align__(8) uint64_t full[NBUF];    // box landed (TMA complete_tx)
+    __shared__ __align__(8) uint64_t empty[NBUF];   // every consumer warp finished reading the box
+    __shared__ int2 org[NBUF];                      // box origin (column, row)
+    __shared__ float4 qv[NBUF];                     // {sin, cos, h} of the view in each buffer
+    __shared__ int ovf[NBUF];                       // footprint larger than the box: use global loads
+    __shared__ int abort_flag_s;
+    volatile int& abort_flag = abort_flag_s;  // set by any thread whose bounded wait gave up
     T* buf = reinterpret_cast<T*>(smem_raw);
 
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+    // Consumer warp w covers an 8 (x) x 4 (y) patch of columns: its lanes then
+    // sample a compact patch of the box (a few rows x ~12 words), which keeps
+    // the shared-memory loads nearly free of bank conflicts even for voxels
+    // larger than a detector pixel; stores remain full 32-byte sectors.
+    const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp == kConsumerWarps;
     const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * ZC;
-    const int x = x0 + tx, y = y0 + ty;
+    const int x = x0 + (warp & 3) * 8 + (lane & 7), y = y0 + ((warp >> 2) & 1) * 4 + (lane >> 3);
+    const int x1 = min(x0 + kTX, g.X) - 1, y1 = min(y0 + kTY, g.Y) - 1;
+    const int zl = min(ZC, g.Zs - z0);  // voxels of this tile in the slab
+    const long long plane = (long long)g.X * g.Y;
+
+    // A tile whose closest column lies outside the reconstruction cylinder has
+    // no voxel to update: write its zeros (unless accumulating) and leave.
+    {
+        const float ax = world_coord(x0, g.xPre, g.vs), bxw = world_coord(x1, g.xPre, g.vs);
+        const float ay = world_coord(y0, g.yPre, g.vs), byw = world_coord(y1, g.yPre, g.vs);
+        const float dx = fmaxf(0.0f, fmaxf(ax, -bxw)), dy = fmaxf(0.0f, fmaxf(ay, -byw));
+        if (dx * dx + dy * dy > g.r2 * 1.0001f + 1.0f) {
+            if (!producer && !accumulate && x < g.X && y < g.Y) {
+                float* out = vol + (long long)z0 * plane + (long long)y * g.X + x;
+                for (int j = 0; j < zl; ++j) out[j * plane] = 0.0f;
+            }
+            return;
+        }
+    }
     const float xw = world_coord(x, g.xPre, g.vs);
     const float yw = world_coord(y, g.yPre, g.vs);
-    const bool live = x < g.X && y < g.Y && in_cylinder(xw, yw, g.r2);
-    const int zl = min(ZC, g.Zs - z0);  // voxels of this tile in the slab
+    const bool live = !producer && x < g.X && y < g.Y && in_cylinder(xw, yw, g.r2);
 
-    float zw[ZC];
+    float zf[ZC];
 #pragma unroll
-    for (int j = 0; j < ZC; ++j) zw[j] = world_coord(z0 + j, g.zPre, g.vs);
-    float acc[ZC];
-#pragma unroll
-    for (int j = 0; j < ZC; ++j) acc[j] = 0.0f;
+    for (int j = 0; j < ZC; ++j) zf[j] = float(g.z_begin + z0 + j);
 
     if (tid == 0) {
-        for (int i = 0; i < kNBuf; ++i) mbar_init(&mbar[i], 1);
+        for (int i = 0; i < NBUF; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], kConsumerWarps);
+        }
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    // corner footprint of view iv -> box origin, then the TMA load (warp 0)
-    // the whole ZC tile is evaluated (voxels past the slab end are discarded
-    // at the store), so the footprint covers all ZC z positions
-    const float zlo = zw[0], zhi = zw[ZC - 1];
-    int issued = 0;  // views whose box load has been issued (tracked by warp 0)
-    auto issue = [&](int iv) {
-        const int b = iv % kNBuf;
-        issued = iv + 1;
-        float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
-        if (lane < 4) {
-            const int cx = min(x0 + (lane & 1) * (kTX - 1), g.X - 1);
-            const int cy = min(y0 + (lane >> 1) * (kTY - 1), g.Y - 1);
+    if (producer) {
+        // ------------------------------------------------------------ producer
+        int iv = 0;
+        for (; iv < n_views && !abort_flag; ++iv) {
+            const int b = iv % NBUF;
+            // the buffer's previous view (iv - NBUF) must have been read by every consumer warp
+            if (iv >= NBUF) {
+                unsigned tries = 0;
+                while (!mbar_try_wait(&empty[b], uint32_t(((iv / NBUF) + 1) & 1))) {
+                    if (++tries > kWaitLimit) {
+                        abort_flag = 1;
+                        break;
+                    }
+                }
+                if (abort_flag) break;
+            }
+            // footprint of the whole ZC tile (voxels past the slab end are evaluated
+            // too and dropped at the store): project the 4 (x, y) corners at both z ends
+            float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
             const float4 q = __ldg(&views[iv]);
-            float U, u;
-            column_geom(world_coord(cx, g.xPre, g.vs), world_coord(cy, g.yPre, g.vs), q.x, q.y, g.D, g.uOff, &U,
-                        &u);
-            const float ui = __fadd_rn(u, g.uPre);
-            float v;
-            const float va = row_coord(zlo, q.z, U, g.vPre, &v);
-            const float vb = row_coord(zhi, q.z, U, g.vPre, &v);
-            umin = umax = ui;
-            vmin = fminf(va, vb);
-            vmax = fmaxf(va, vb);
-        }
+            if (lane < 4) {
+                const int cx = (lane & 1) ? x1 : x0;
+                const int cy = (lane >> 1) ? y1 : y0;
+                float U, u;
+                column_geom(world_coord(cx, g.xPre, g.vs), world_coord(cy, g.yPre, g.vs), q.x, q.y, g.D, g.uOff,
+                            &U, &u);
+                const RowLine rl = row_line(U, q.z, g.zpv, g.vs, g.vPre);
+                const float va = row_at(rl, zf[0]), vb = row_at(rl, zf[ZC - 1]);
+                umin = umax = __fadd_rn(u, g.uPre);
+                vmin = fminf(va, vb);
+                vmax = fmaxf(va, vb);
+            }
 #pragma unroll
-        for (int o = 1; o < 4; o <<= 1) {
-            umin = fminf(umin, __shfl_xor_sync(0xffffffffu, umin, o));
-            umax = fmaxf(umax, __shfl_xor_sync(0xffffffffu, umax, o));
-            vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
-            vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+            for (int o = 1; o < 4; o <<= 1) {
+                umin = fminf(umin, __shfl_xor_sync(0xffffffffu, umin, o));
+                umax = fmaxf(umax, __shfl_xor_sync(0xffffffffu, umax, o));
+                vmin = fminf(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+                vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+            }
+            if (lane == 0) {
+                // clamp non-finite / huge values so the integer conversions stay defined
+                umin = fminf(fmaxf(umin, -1.0e6f), 1.0e6f); umax = fminf(fmaxf(umax, -1.0e6f), 1.0e6f);
+                vmin = fminf(fmaxf(vmin, -1.0e6f), 1.0e6f); vmax = fminf(fmaxf(vmax, -1.0e6f), 1.0e6f);
+                const int uo = ((int(floorf(umin)) - 2) >> 3) << 3;   // 16-byte aligned column
+                const int vo = int(floorf(vmin)) - 2;
+                org[b] = make_int2(uo, vo);
+                qv[b] = q;
+                ovf[b] = (int(floorf(umax)) + 3 - uo > bx.BU) || (int(floorf(vmax)) + 3 - vo > bx.BV);
+                mbar_expect_tx(&full[b], uint32_t(bx.BU) * bx.BV * sizeof(T));
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                tma_load_3d(buf + size_t(b) * bx.buf_elems, &map, uo, vo, iv, &full[b]);
+            }
+            __syncwarp();
         }
-        if (lane == 0) {
-            // clamp non-finite / huge values so the integer conversions stay defined
-            umin = fminf(fmaxf(umin, -1.0e6f), 1.0e6f); umax = fminf(fmaxf(umax, -1.0e6f), 1.0e6f);
-            vmin = fminf(fmaxf(vmin, -1.0e6f), 1.0e6f); vmax = fminf(fmaxf(vmax, -1.0e6f), 1.0e6f);
-            const int uo = ((int(floorf(umin)) - 2) >> 3) << 3;   // 16-byte aligned column
-            const int vo = int(floorf(vmin)) - 2;
-            org[b] = make_int2(uo, vo);
-            ovf[b] = (int(floorf(umax)) + 3 - uo > bx.BU) || (int(floorf(vmax)) + 3 - vo > bx.BV);
-            mbar_expect_tx(&mbar[b], uint32_t(bx.BU) * bx.BV * sizeof(T));
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            tma_load_3d(buf + size_t(b) * bx.buf_elems, &map, uo, vo, iv, &mbar[b]);
+        __syncthreads();
+        if (abort_flag && lane == 0) {
+            atomicAdd(&g_wait_timeouts, 1u);
+            // bounded drain of every issued box not yet known to have landed before the
+            // CTA's shared memory goes away (the last NBUF issued views)
+            for (int i = max(0, iv - NBUF); i < iv; ++i) {
+                unsigned tries = 0;
+                while (!mbar_try_wait(&full[i % NBUF], uint32_t((i / NBUF) & 1)) && ++tries < kWaitLimit) {
+                }
+            }
         }
-    };
+        return;
+    }
 
-    if (warp == 0)
-        for (int i = 0; i < kNBuf - 1 && i < n_views; ++i) issue(i);
-
-    int abort_iv = n_views;
+    // -------------------------------------------------------------- consumers
+    float acc[ZC];
+#pragma unroll
+    for (int j = 0; j < ZC; ++j) acc[j] = 0.0f;
     for (int iv = 0; iv < n_views; ++iv) {
-        const int b = iv % kNBuf;
-        if (warp == 0 && iv + kNBuf - 1 < n_views) issue(iv + kNBuf - 1);
+        const int b = iv % NBUF;
         // bounded wait for the box of view iv
         unsigned tries = 0;
-        while (!mbar_try_wait(&mbar[b], uint32_t((iv / kNBuf) & 1))) {
+        while (!mbar_try_wait(&full[b], uint32_t((iv / NBUF) & 1))) {
             if (++tries > kWaitLimit) {
                 abort_flag = 1;
                 break;
             }
         }
-        if (live && !abort_flag) {
-            const float4 q = __ldg(&views[iv]);
+        if (abort_flag) break;
+        if (live) {
+            const float4 q = qv[b];
             float U, u;
             column_geom(xw, yw, q.x, q.y, g.D, g.uOff, &U, &u);
             if (u >= g.lbU && u <= g.ubU) {
@@ -195,36 +249,49 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant
                 const float ui = __fadd_rn(u, g.uPre);
                 const int u0 = int(ui);
                 const float fu = __fsub_rn(ui, float(u0));
-                const int2 o = org[b];
-                float v;
-                const float vi_first = row_coord(zw[0], q.z, U, g.vPre, &v);
-                const float vi_last = row_coord(zw[ZC - 1], q.z, U, g.vPre, &v);
-                // strictly inside the row bounds (half-pixel margin): every voxel of the column passes the
-                // per-voxel test, so the fast path and the checked path take the same decisions
-                const bool all_rows =
-                    fminf(vi_first, vi_last) >= 0.5f && fmaxf(vi_first, vi_last) <= bx.vi_hi - 0.5f;
+                const RowLine rl = row_line(U, q.z, g.zpv, g.vs, g.vPre);
+                const float vf = row_at(rl, zf[0]), vl = row_at(rl, zf[ZC - 1]);
                 if (!ovf[b]) {
+                    const int2 o = org[b];
                     const T* col = buf + size_t(b) * bx.buf_elems + (u0 - o.x) - o.y * bx.BU;
+                    const int BU = bx.BU;
+                    // strictly inside the row bounds (half-pixel margin): every voxel of the column passes
+                    // the per-voxel test, so this loop and the checked one take the same decisions
+                    if (fminf(vf, vl) >= 0.5f && fmaxf(vf, vl) <= g.vi_hi - 0.5f) {
 #pragma unroll
-                    for (int j = 0; j < ZC; ++j) {
-                        const float vi = row_coord(zw[j], q.z, U, g.vPre, &v);
-                        if (all_rows || (v >= g.lbV && v <= g.ubV)) {
+                        for (int j = 0; j < ZC; ++j) {
+                            const float vi = row_at(rl, zf[j]);
                             const int v0 = int(vi);
                             const float fv = __fsub_rn(vi, float(v0));
-                            const T* r0 = col + v0 * bx.BU;
+                            const T* r0 = col + v0 * BU;
                             const float p00 = sval(r0[0]), p01 = sval(r0[1]);
-                            const float p10 = sval(r0[bx.BU]), p11 = sval(r0[bx.BU + 1]);
+                            const float p10 = sval(r0[BU]), p11 = sval(r0[BU + 1]);
                             const float a = fmaf(fu, p01 - p00, p00);
                             const float c = fmaf(fu, p11 - p10, p10);
                             acc[j] = fmaf(w, fmaf(fv, c - a, a), acc[j]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < ZC; ++j) {
+                            const float vi = row_at(rl, zf[j]);
+                            if (row_ok(vi, g.vi_hi)) {
+                                const int v0 = int(vi);
+                                const float fv = __fsub_rn(vi, float(v0));
+                                const T* r0 = col + v0 * BU;
+                                const float p00 = sval(r0[0]), p01 = sval(r0[1]);
+                                const float p10 = sval(r0[BU]), p11 = sval(r0[BU + 1]);
+                                const float a = fmaf(fu, p01 - p00, p00);
+                                const float c = fmaf(fu, p11 - p10, p10);
+                                acc[j] = fmaf(w, fmaf(fv, c - a, a), acc[j]);
+                            }
                         }
                     }
                 } else {
                     const T* col = proj + (long long)iv * g.view_stride + u0;
 #pragma unroll
                     for (int j = 0; j < ZC; ++j) {
-                        const float vi = row_coord(zw[j], q.z, U, g.vPre, &v);
-                        if (v >= g.lbV && v <= g.ubV) {
+                        const float vi = row_at(rl, zf[j]);
+                        if (row_ok(vi, g.vi_hi)) {
                             const int v0 = int(vi);
                             const float fv = __fsub_rn(vi, float(v0));
                             const T* r0 = col + (long long)v0 * g.W;
@@ -236,27 +303,12 @@ __global__ void __launch_bounds__(kTX * kTY) bp_tma_kernel(const __grid_constant
                 }
             }
         }
-        __syncthreads();
-        if (abort_flag) {
-            abort_iv = iv;
-            break;
-        }
+        // this warp is done with the box of view iv
+        __syncwarp();
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b])) : "memory");
     }
-    if (abort_flag) {
-        if (tid == 0) {
-            atomicAdd(&g_wait_timeouts, 1u);
-            // bounded drain of the boxes issued but not consumed (views abort_iv .. issued-1)
-            // before the CTA's shared memory goes away
-            for (int i = abort_iv; i < issued; ++i) {
-                unsigned tries = 0;
-                while (!mbar_try_wait(&mbar[i % kNBuf], uint32_t((i / kNBuf) & 1)) && ++tries < kWaitLimit) {
-                }
-            }
-        }
-        return;
-    }
-    if (x >= g.X || y >= g.Y) return;
-    const long long plane = (long long)g.X * g.Y;
+    __syncthreads();
+    if (abort_flag || x >= g.X || y >= g.Y) return;
     float* out = vol + (long long)z0 * plane + (long long)y * g.X + x;
 #pragma unroll
     for (int j = 0; j < ZC; ++j) {
@@ -288,7 +340,10 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     // largest |(x, y)| of any grid column
     const double xa = std::max(std::fabs((0 - g.xPre) * vs), std::fabs((g.X - 1 - g.xPre) * vs));
     const double ya = std::max(std::fabs((0 - g.yPre) * vs), std::fabs((g.Y - 1 - g.yPre) * vs));
-    const double R = std::sqrt(xa * xa + ya * ya);
+    // only tiles that reach into the cylinder load boxes: their corners lie
+    // within the cylinder radius plus one tile diagonal of the axis
+    const double T0 = std::sqrt(std::pow((kTX - 1) * vs, 2) + std::pow((kTY - 1) * vs, 2));
+    const double R = std::min(std::sqrt(xa * xa + ya * ya), double(std::sqrt(g.r2)) + T0);
     if (R >= 0.9 * D) return false;
     const double Umax = D / (D - R), dU = Umax * Umax / D;
     const double T = std::sqrt(std::pow((kTX - 1) * vs, 2) + std::pow((kTY - 1) * vs, 2));
@@ -297,8 +352,13 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     const double zabs =
         std::max(std::fabs((0 - g.zPre) * vs), std::fabs((g.Zs + ZC - 1 - g.zPre) * vs)) + hmax;
     const double vext = (ZC - 1) * vs * Umax + zabs * dU * T;
+    // row stride: an odd number of 16-byte chunks, so that consecutive box rows
+    // start in different shared-memory banks (a multiple of 128 bytes would put
+    // the same column of every row in one bank)
+    const int chunk = 16 / esize;
     int BU = int(std::ceil(uext)) + 12;
-    BU = (BU + 7) / 8 * 8;
+    BU = (BU + chunk - 1) / chunk * chunk;
+    if ((BU / chunk) % 2 == 0) BU += chunk;
     const int BV = int(std::ceil(vext)) + 6;
     if (BU > 256 || BV > 256) return false;
     b->BU = BU;
@@ -327,14 +387,16 @@ int launch_t(const T* proj, CUtensorMapDataType dt, const float4* views, int n_v
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return CTB_ERR_UNSUPPORTED;
-    const size_t smem = size_t(kNBuf) * bx.buf_elems * sizeof(T);
-    auto kern = bp_tma_kernel<T, ZC>;
+    // three box buffers when three CTAs still fit an SM's shared memory, else two
+    const size_t per_buf = size_t(bx.buf_elems) * sizeof(T);
+    const int nbuf = (3 * (3 * per_buf + 1024) <= 227 * 1024) ? 3 : 2;
+    const size_t smem = size_t(nbuf) * per_buf;
     if (smem > 200 * 1024) return CTB_ERR_UNSUPPORTED;
+    auto kern = nbuf == 3 ? bp_tma_kernel<T, ZC, 3> : bp_tma_kernel<T, ZC, 2>;
     CTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    dim3 block(kTX, kTY, 1);
     dim3 grid((g.X + kTX - 1) / kTX, (g.Y + kTY - 1) / kTY, (g.Zs + ZC - 1) / ZC);
     if (grid.y > 65535 || grid.z > 65535) return CTB_ERR_UNSUPPORTED;
-    kern<<<grid, block, smem, s>>>(map, proj, views, n_views, g, bx, vol, accumulate);
+    kern<<<grid, kThreads, smem, s>>>(map, proj, views, n_views, g, bx, vol, accumulate);
     return cuda_status(cudaGetLastError(), "bp_tma_kernel launch");
 }
 

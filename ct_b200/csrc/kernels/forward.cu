@@ -76,17 +76,18 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
             else if (u0 + 1 == c) bu = fu;
             else continue;
             const float w = __fmul_rn(__fmul_rn(U, U), g.load_scale);
-            // rows: vi = vPre - (zw + h) U in [r-1, r+1)  ->  z range
+            // rows: vi(z) = c0 + z mdv in [r-1, r+1)  ->  z range (mdv < 0)
             const float* col = volz + ((long long)x * g.Y + y) * g.Zs;
-            const double zlo = ((double(g.vPre) - (r + 1)) / U - h) / g.vs + g.zPre;
-            const double zhi = ((double(g.vPre) - (r - 1)) / U - h) / g.vs + g.zPre;
+            const RowLine rl = row_line(U, h, g.zpv, g.vs, g.vPre);
+            const double dv = -double(rl.mdv);
+            // (box z index = slab-local z + z_begin)
+            const double zlo = (double(rl.c0) - (r + 1)) / dv - g.z_begin;
+            const double zhi = (double(rl.c0) - (r - 1)) / dv - g.z_begin;
             const int z0 = max(0, int(floor(zlo)) - 1);
             const int z1 = min(g.Zs - 1, int(ceil(zhi)) + 1);
             for (int z = z0; z <= z1; ++z) {
-                const float zw = world_coord(z, g.zPre, g.vs);
-                float v;
-                const float vi = row_coord(zw, h, U, g.vPre, &v);
-                if (!(v >= g.lbV && v <= g.ubV)) continue;
+                const float vi = row_at(rl, float(g.z_begin + z));
+                if (!row_ok(vi, g.vi_hi)) continue;
                 const int v0 = int(vi);
                 const float fv = __fsub_rn(vi, float(v0));
                 float bv;

@@ -29,10 +29,26 @@ __device__ __forceinline__ void column_geom(float xw, float yw, float sn, float 
     *u = __fmul_rn(t, *U);
 }
 
-// Detector row coordinate of a voxel: vi = (-1)*((z + h) * U) + H/2 (:1008, :1014).
-__device__ __forceinline__ float row_coord(float zw, float h, float U, float vPre, float* v) {
-    *v = __fmul_rn(__fadd_rn(zw, h), U);
-    return __fadd_rn(-*v, vPre);
+// Detector row coordinate of a voxel, vi = H/2 - (zw + h) U (:1008, :1014),
+// as a line in the box voxel index z: vi(z) = fma(z, mdv, c0) with
+// zw = (z - zPre) vs, mdv = -vs U and c0 = H/2 - (h - zPre vs) U. One fused
+// multiply-add per voxel; the backprojectors and the forward projector all use
+// exactly this form so that they take the same row decisions.
+struct RowLine {
+    float mdv, c0;
+};
+
+__device__ __forceinline__ RowLine row_line(float U, float h, float zpv, float vs, float vPre) {
+    RowLine r;
+    r.mdv = -__fmul_rn(vs, U);
+    r.c0 = fmaf(-__fsub_rn(h, zpv), U, vPre);
+    return r;
 }
+
+__device__ __forceinline__ float row_at(const RowLine& r, float zf) { return fmaf(zf, r.mdv, r.c0); }
+
+// A row coordinate is inside the detector when 0 <= vi <= H - 1.1
+// (the v bounds of :927-928 and :1011 expressed on vi).
+__device__ __forceinline__ bool row_ok(float vi, float vi_hi) { return vi >= 0.0f && vi <= vi_hi; }
 
 }  // namespace ctb

@@ -147,24 +147,28 @@ def log(*a):
     print("[bench]", *a, file=sys.stderr, flush=True)
 
 
-def fp64_reference_slices(raw, cfg, geom, det, grid, z0, z1):
-    """FP64 oracle reconstruction of box slices [z0, z1) from only the detector rows they touch."""
+def oracle_rows(raw, geom, det, grid, z0, z1):
+    """The detector rows that box slices [z0, z1) touch in any view, copied to the host."""
     import torch
-
-    from oracle import oracle as orc
-    orc.build()
     V, H, W = raw.shape
     vs = grid.voxel_pitch
     zpre = grid.z_size / 2.0 - grid.z_from
     zw = np.array([(z0 - zpre) * vs, (z1 - 1 - zpre) * vs])
-    R = float(det.radius)
-    D = float(det.fcd)
-    U = np.array([D / (D + R), D / (D - R)])
-    v = np.outer(zw, U).ravel()
-    vpre = H / 2.0
-    r0 = max(0, int(math.floor(vpre - v.max())) - 2)
-    r1 = min(H, int(math.floor(vpre - v.min())) + 3)
-    rows = raw[:, r0:r1, :].to(torch.int32).cpu().numpy().astype(np.uint16)
+    R, D = float(det.radius), float(det.fcd)
+    v = np.outer(zw, np.array([D / (D + R), D / (D - R)])).ravel()
+    r0 = max(0, int(math.floor(H / 2.0 - v.max())) - 2)
+    r1 = min(H, int(math.floor(H / 2.0 - v.min())) + 3)
+    return r0, raw[:, r0:r1, :].to(torch.int32).cpu().numpy().astype(np.uint16)
+
+
+def fp64_reference_slices(rows, cfg, geom, det, grid, z0, z1):
+    """FP64 oracle reconstruction of box slices [z0, z1) from only the detector rows they touch."""
+    from oracle import oracle as orc
+    orc.build()
+    r0, rows = rows
+    V, _, W = rows.shape
+    H = det.height
+    vs = grid.voxel_pitch
     g = orc.custom_geom(W, H, float(det.fcd), (grid.x_size, grid.y_size, grid.z_size), vs)
     ref = orc.f64_slices(rows, r0, H, geom.angles(), np.zeros(V), 1.0, FILTERS[cfg["filter"]], g, z0, z1)
     return ref  # (x, y, z1 - z0)
@@ -185,8 +189,11 @@ def dist_setup():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1 and not dist.is_initialized():
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:  # host-only runs of the rank plumbing
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     return world, rank, local
 
 
@@ -201,9 +208,168 @@ def max_over_ranks(x: float, world: int) -> float:
     import torch.distributed as dist
     if world == 1:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def scan_seed(rank: int) -> int:
+    """Each rank reconstructs its own object (weak scaling, no data-path collective)."""
+    return 1000 + rank
+
+
+def whole_job_gups(voxel_views_per_rank: float, world: int, ms_per_step: float) -> float:
+    """Whole-job throughput: the units all ranks processed over the max-over-ranks step time."""
+    return voxel_views_per_rank * world / (ms_per_step * 1e-3) / 1e9
+
+
+# ---------------------------------------------------------------- batch (C5)
+def batch_c5(n_scans=32, seed=5, store="fp16", reps=3):
+    """C5: 32 independent scans, detector W and H ~ U[128, 768], views ~ U[90, 720], volume edge ~ U[96, 384]
+    float32, SOD ~ U[300, 700] mm, magnification ~ U[1.5, 2.5], 5-25 seeded ellipsoids each. Aggregate GUPS of
+    the persistent graph-captured batch against launching the scans one by one."""
+    import torch
+
+    from ct_b200 import ops, synth
+    from ct_b200 import _lib as L
+    rng = np.random.default_rng(seed)
+    st = {"fp16": L.FP16, "bf16": L.BF16, "fp32": L.FP32}[store]
+    scans, units = [], 0.0
+    for i in range(n_scans):
+        W, H = int(rng.integers(128, 769)), int(rng.integers(128, 769))
+        V = int(rng.integers(90, 721))
+        edge = int(rng.integers(96, 385))
+        sod = float(rng.uniform(300, 700))
+        mag = float(rng.uniform(1.5, 2.5))
+        pitch = 0.2
+        geom = synth.ScanGeometry(V, W, H, pitch, sod, sod * mag)
+        sc = synth.make_scan(geom, int(rng.integers(5, 26)), seed=seed * 1000 + i)
+        det, _ = ops.detector(W, H, float(np.float32(geom.fcd_px)))
+        # the volume spans the detector's field of view at the detector pixel pitch scaled to the edge
+        vs = float(W) / edge
+        grid = ops.custom_grid(det, (edge, edge, edge), vs)
+        vol = torch.empty((edge, edge, edge), device="cuda")
+        scans.append(dict(raw=sc.images, angles_deg=geom.angles(), heights_px=None, det=det, grid=grid,
+                          filter=int(rng.integers(0, 3)), pad=1, vol=vol))
+        units += float(edge) ** 3 * V
+    b = ops.Batch(scans, st)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_graph = timed(b.run)
+    ms_seq = timed(b.run_sequential)
+    out = {"scans": n_scans, "voxel_views": units, "storage": store,
+           "graph_persistent": {"ms": ms_graph, "gups": units / (ms_graph * 1e-3) / 1e9},
+           "one_by_one": {"ms": ms_seq, "gups": units / (ms_seq * 1e-3) / 1e9},
+           "speedup": ms_seq / ms_graph, "autotune": b.tuning()}
+    del b, scans
+    torch.cuda.empty_cache()
+    return out
+
+
+# ------------------------------------------------------- differentiation (C4)
+def voxelise_gpu(ellipsoids, edge, voxel_mm):
+    """Phantom density at the voxel centres of an edge^3 grid centred on the axis, (Z, Y, X) float32."""
+    import torch
+    c = (torch.arange(edge, device="cuda", dtype=torch.float64) - edge / 2.0) * voxel_mm
+    out = torch.zeros((edge, edge, edge), device="cuda", dtype=torch.float32)
+    Z, Y = torch.meshgrid(c, c, indexing="ij")
+    for E in np.asarray(ellipsoids, np.float64):
+        R = torch.tensor(E[6:15].reshape(3, 3), device="cuda", dtype=torch.float64)
+        for xi in range(0, edge, 64):  # chunks of x keep the temporaries small
+            X = c[xi:xi + 64]
+            P = torch.stack(torch.broadcast_tensors(X[None, None, :], Y[:, :, None], Z[:, :, None]), -1)
+            q = ((P - torch.tensor(E[:3], device="cuda")) @ R) / torch.tensor(E[3:6], device="cuda")
+            out[:, :, xi:xi + 64] += torch.where((q * q).sum(-1) <= 1.0, float(E[15]), 0.0).float()
+    return out
+
+
+def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
+    """C4: matched forward projector A and backprojector A^T on a 512^3 float32 volume, 360 views of
+    512x512. Dot-product test <Ax, y> = <x, A^T y> with seeded Gaussian x, y; central finite differences of
+    f(x) = ||Ax - p||^2 on 64 random voxels against 2 A^T (Ax - p) (A(x +- eps e_i) = Ax +- eps A e_i, with
+    A e_i projected from a one-slice slab holding the voxel); then 20 steepest-descent iterations with exact
+    line search from the FDK reconstruction of a 20-ellipsoid phantom with Poisson noise at 1e4 photons."""
+    import torch
+
+    from ct_b200 import ops, synth
+    from ct_b200 import _lib as L
+    geom = synth.ScanGeometry(views, det, det, 0.4, 500.0, 1000.0)
+    d, _ = ops.detector(det, det, float(np.float32(geom.fcd_px)))
+    grid = ops.custom_grid(d, (edge, edge, edge), 1.0)
+    ang = geom.angles()
+    out = {"volume": [edge] * 3, "views": views, "detector": [det, det]}
+    t0 = time.perf_counter()
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.randn((edge, edge, edge), device="cuda", generator=g)
+    y = torch.randn((views, det, det), device="cuda", generator=g)
+    Ax = ops.forward_project(x, ang, None, d, grid)
+    Aty = ops.backproject(y, ang, None, d, grid)
+    lhs, rhs = float((Ax.double() * y.double()).sum()), float((x.double() * Aty.double()).sum())
+    out["dot_test_rel"] = abs(lhs - rhs) / max(abs(lhs), abs(rhs))
+    del Ax, Aty, y
+    # data: noisy analytic phantom, line integrals in detector-pixel units
+    scan = synth.make_scan(geom, 20, seed=seed, photons=1e4)
+    p = -torch.log(torch.clamp(scan.images.float(), min=1.0) / 65535.0) / (0.02 * geom.pixel_eff)
+    # FDK start (ramlak, FP32), rescaled to the data by least squares
+    filt = ops.filter_projections(scan.images, d, L.RAMLAK, 1, L.FP32)
+    x = ops.backproject(filt, ang, None, d, grid)
+    del filt
+    Ax = ops.forward_project(x, ang, None, d, grid)
+    c = float((Ax.double() * p.double()).sum() / (Ax.double() * Ax.double()).sum())
+    x.mul_(c)
+    r = Ax.mul_(c).sub_(p)
+    # finite differences on 64 voxels
+    grad = 2.0 * ops.backproject(r, ang, None, d, grid)
+    rng = np.random.default_rng(seed)
+    eps, worst = 1.0, 0.0
+    for _ in range(64):
+        k, j, i = (int(rng.integers(edge // 4, 3 * edge // 4)) for _ in range(3))
+        slab = torch.zeros((1, edge, edge), device="cuda")
+        slab[0, j, i] = 1.0
+        Ae = ops.forward_project(slab, ang, None, d, grid, k, k + 1).double()
+        rd = r.double()
+        fp = float(((rd + eps * Ae) ** 2).sum())
+        fm = float(((rd - eps * Ae) ** 2).sum())
+        fd = (fp - fm) / (2 * eps)
+        gi = float(grad[k, j, i])
+        worst = max(worst, abs(fd - gi) / max(abs(fd), 1e-12))
+    out["fd_max_rel_err_64_voxels"] = worst
+    # steepest descent with exact line search on the quadratic
+    res0 = float(r.double().norm() / p.double().norm())
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    for _ in range(iters):
+        gk = 2.0 * ops.backproject(r, ang, None, d, grid)
+        Ag = ops.forward_project(gk, ang, None, d, grid)
+        alpha = float((gk.double() ** 2).sum() / (2.0 * (Ag.double() ** 2).sum()))
+        x.sub_(alpha * gk)
+        r.sub_(alpha * Ag)
+        del gk, Ag
+    torch.cuda.synchronize()
+    t_it = (time.perf_counter() - t1) / iters
+    res = float(r.double().norm() / p.double().norm())
+    # error to the voxelised phantom (after the best scalar fit of the units)
+    truth = voxelise_gpu(scan.ellipsoids, edge, geom.pixel_eff)
+    xs = x.double()
+    s_fit = float((xs * truth).sum() / (xs * xs).sum())
+    out.update({"data_residual_rel_start": res0, "data_residual_rel_after": res, "iterations": iters,
+                "rel_l2_to_phantom_after": float((s_fit * xs - truth).norm() / truth.norm()),
+                "seconds_per_iteration": t_it, "seconds_total": time.perf_counter() - t0})
+    del x, r, p, truth, scan
+    torch.cuda.empty_cache()
+    return out
 
 
 # ------------------------------------------------------------------ our arm
@@ -223,7 +389,7 @@ def run_ours(args):
     store = {"fp16": L.FP16, "bf16": L.BF16, "fp32": L.FP32}[args.store]
 
     # independent scan per rank (weak scaling: each rank reconstructs its own object)
-    scan = synth.make_scan(geom, cfg["n_ell"], seed=1000 + rank, photons=cfg["photons"], n_small=cfg["n_small"])
+    scan = synth.make_scan(geom, cfg["n_ell"], seed=scan_seed(rank), photons=cfg["photons"], n_small=cfg["n_small"])
     raw = scan.images
     angles = geom.angles()
     det, _ = ops.detector(W, H, geom.fcd_px)
@@ -281,7 +447,7 @@ def run_ours(args):
     log(f"scan ready: {V} views {W}x{H} -> {X}x{Y}x{Z}")
     main, centre = timed(store, args.steps, args.warmup)
     ms_per_step = main["total_ms"] / args.steps
-    value = units * world / (ms_per_step * 1e-3) / 1e9
+    value = whole_job_gups(units, world, ms_per_step)
     log(f"{args.store}: {ms_per_step:.1f} ms/step, {value:.1f} GUPS, filter {main['filter_ms']:.1f} ms, "
         f"bp {main['bp_ms']:.1f} ms, clocks {main['clocks']}")
 
@@ -290,19 +456,16 @@ def run_ours(args):
     if store != L.FP32 and not args.skip_fp32:
         r32, centre32 = timed(L.FP32, max(2, args.steps // 2), 1)
         ms32 = r32["total_ms"] / max(2, args.steps // 2)
-        fp32 = {"value": units * world / (ms32 * 1e-3) / 1e9, "ms_per_step": ms32, "bp_ms": r32["bp_ms"],
+        fp32 = {"value": whole_job_gups(units, world, ms32), "ms_per_step": ms32, "bp_ms": r32["bp_ms"],
                 "filter_ms": r32["filter_ms"]}
         log(f"fp32: {fp32}")
 
-    # accuracy of the volumes on the two central slices vs the FP64 oracle
+    # the central slices' FP64-oracle accuracy is computed in the CPU leg below
     acc = None
-    if rank == 0 and not args.skip_accuracy:
-        zc = Z // 2
-        ref = fp64_reference_slices(raw, cfg, geom, det, grid, zc - 1, zc + 1)
-        acc = {"slices": [zc - 1, zc + 1], args.store: accuracy(centre, ref)}
-        if centre32 is not None:
-            acc["fp32"] = accuracy(centre32, ref)
-        log(f"accuracy: {acc}")
+    zc = Z // 2
+    rows_for_oracle = None
+    if rank == 0 and world == 1 and not args.skip_cpu and not args.skip_accuracy:
+        rows_for_oracle = oracle_rows(raw, geom, det, grid, zc - 1, zc + 1)
 
     # end to end through the C ABI facade: pinned host u16 -> pinned host float volume
     e2e = None
@@ -328,12 +491,21 @@ def run_ours(args):
         barrier(world)
         tm = v.timings()
         sec = max_over_ranks(float(np.mean(ts)), world)
-        e2e = {"value": units * world / sec / 1e9, "unit": "GUPS", "seconds": sec,
+        e2e = {"value": whole_job_gups(units, world, sec * 1e3), "unit": "GUPS", "seconds": sec,
                "h2d_bytes_per_step": int(V * H * W * 2), "d2h_bytes_per_step": int(X * Y * Z * 4),
                "stages_s": {"upload_exposed": tm.upload_s, "filter": tm.filter_s, "backproject": tm.backproject_s,
                             "download_exposed": tm.download_s}}
         del v, host_in, host_out
         log(f"e2e: {e2e}")
+
+    batch = None
+    if not args.skip_batch and args.config == "c3":
+        batch = batch_c5(store=args.store)
+        log(f"batch c5: {batch}")
+    grad = None
+    if not args.skip_gradient and args.config == "c3":
+        grad = gradient_c4()
+        log(f"gradient c4: {grad}")
 
     peaks, peak_kind = measured_peaks()
     clock_mhz = main["clocks"].get("sm_mhz") or peaks.get("sm_max_mhz", 1965.0)
@@ -365,6 +537,8 @@ def run_ours(args):
         "fp32": fp32,
         "mixed_over_fp32": (value / fp32["value"]) if fp32 else None,
         "accuracy_vs_fp64": acc,
+        "batch_c5": batch,
+        "gradient_c4": grad,
         "e2e": e2e,
         "roofline": roofline,
         "roofline_filter": roofline_filter,
@@ -372,9 +546,18 @@ def run_ours(args):
         "clocks": main["clocks"],
     }
     if rank == 0 and world == 1 and not args.skip_cpu:
+        # CPU leg: the reference's CPU path on a bounded sample (baseline) and the FP64
+        # oracle on the central slices (accuracy of this run's volumes)
         sel = np.linspace(0, V - 1, 8).astype(int)
         imgs_sel = torch.stack([raw[int(i)] for i in sel]).to(torch.int32).cpu().numpy().astype(np.uint16)
         line["cpu_baseline"] = cpu_baseline(cfg, imgs_sel, angles[sel], V)
+        if rows_for_oracle is not None:
+            ref = fp64_reference_slices(rows_for_oracle, cfg, geom, det, grid, zc - 1, zc + 1)
+            acc = {"slices": [zc - 1, zc + 1], args.store: accuracy(centre, ref)}
+            if centre32 is not None:
+                acc["fp32"] = accuracy(centre32, ref)
+            line["accuracy_vs_fp64"] = acc
+            log(f"accuracy: {acc}")
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -437,6 +620,8 @@ def main():
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
+    ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--skip-gradient", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)

@@ -39,6 +39,12 @@ class Grid(ctypes.Structure):
         return (self.x_to - self.x_from, self.y_to - self.y_from, self.z_to - self.z_from)
 
 
+class Scan(ctypes.Structure):
+    _fields_ = [("raw", ctypes.c_void_p), ("raw_type", ctypes.c_int32), ("n_views", ctypes.c_int32),
+                ("angles_deg", ctypes.c_void_p), ("height_offsets_px", ctypes.c_void_p), ("det", Detector),
+                ("grid", Grid), ("filter", ctypes.c_int32), ("pad", ctypes.c_int32), ("vol", ctypes.c_void_p)]
+
+
 class Timings(ctypes.Structure):
     _fields_ = [("upload_s", ctypes.c_double), ("filter_s", ctypes.c_double), ("backproject_s", ctypes.c_double),
                 ("download_s", ctypes.c_double), ("total_s", ctypes.c_double), ("voxel_views", ctypes.c_double)]
@@ -69,6 +75,11 @@ SIGNATURES = {
     "ctb_set_skip_projections": (I, [P, ctypes.c_uint]),
     "ctb_set_device": (I, [P, I]),
     "ctb_set_gpu_spare_memory": (I, [P, Z]),
+    "ctb_set_devices": (I, [P, P, I]),
+    "ctb_set_gpu_coefficients": (I, [P, D, D]),
+    "ctb_get_gpu_weights": (I, [P, P, I, P]),
+    "ctb_gpu_weights_from": (I, [P, P, I, D, D, P]),
+    "ctb_split_slices": (I, [P, I, I, P]),
     "ctb_set_precision": (I, [P, I]),
     "ctb_set_pad": (I, [P, I]),
     "ctb_set_grid": (I, [P, I, I, I, F]),
@@ -86,6 +97,14 @@ SIGNATURES = {
     "ctb_stop": (None, [P]),
     "ctb_get_timings": (I, [P, P]),
     "ctb_phantom_project": (I, [P, I, P, P, I, I, I, D, D, D, P, P]),
+    "ctb_read_volume_info": (I, [ctypes.c_char_p, P, P, P, P, P]),
+    "ctb_load_volume": (I, [ctypes.c_char_p, I, I, I, I, I, I, Z, I, I, I, P]),
+    "ctb_get_cross_section": (I, [P, I, I, P, P, P]),
+    "ctb_batch_create": (I, [P, I, P, I, P]),
+    "ctb_batch_run": (I, [P, P]),
+    "ctb_batch_run_sequential": (I, [P, P]),
+    "ctb_batch_tuning": (I, [P, P, P, P, P]),
+    "ctb_batch_destroy": (None, [P]),
 }
 
 _lib = None

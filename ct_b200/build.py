@@ -38,10 +38,13 @@ SOURCES = [
     "host/image_io.cpp",
     "host/reconstructor.cpp",
     "host/volume_io.cpp",
+    "host/tables.cpp",
+    "host/batch.cpp",
+    "host/volume_reader.cpp",
     "capi.cpp",
     "noalloc.cu",
 ]
-HEADERS = ["ctb_internal.h", "host/reconstructor.h", "host/image_io.h", "kernels/geom.cuh"]
+HEADERS = ["ctb_internal.h", "host/reconstructor.h", "host/image_io.h", "host/autotune.h", "kernels/geom.cuh"]
 
 
 def _obj(src: str) -> str:

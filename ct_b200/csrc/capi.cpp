@@ -5,11 +5,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <map>
 #include <mutex>
 #include <new>
 #include <string>
-#include <tuple>
 
 #include "ctb_internal.h"
 #include "host/reconstructor.h"
@@ -19,48 +17,6 @@ struct ctb_ctx {
 };
 
 namespace {
-
-// Filter tables cached per (device, W, pad, filter) for the operator layer.
-struct TableKey {
-    int dev, W, pad, filter;
-    bool operator<(const TableKey& o) const {
-        return std::tie(dev, W, pad, filter) < std::tie(o.dev, o.W, o.pad, o.filter);
-    }
-};
-struct Tables {
-    int M = 0, logM = 0;
-    float2* tw = nullptr;
-    float* K = nullptr;
-};
-std::mutex g_tables_mtx;
-std::map<TableKey, Tables> g_tables;
-
-int get_tables(int W, int pad, int filter, cudaStream_t s, Tables* out) {
-    int dev = 0;
-    CTB_CUDA_TRY(cudaGetDevice(&dev));
-    std::lock_guard<std::mutex> lk(g_tables_mtx);
-    const TableKey key{dev, W, pad, filter};
-    auto it = g_tables.find(key);
-    if (it != g_tables.end()) {
-        *out = it->second;
-        return CTB_OK;
-    }
-    Tables t;
-    t.M = ctb::filter_transform_length(W, pad);
-    if (t.M == 0) {
-        ctb::set_global_error("detector width exceeds the largest supported FFT length");
-        return CTB_ERR_UNSUPPORTED;
-    }
-    while ((1 << t.logM) < t.M) ++t.logM;
-    CTB_CUDA_TRY(cudaMalloc(&t.tw, sizeof(float2) * t.M));
-    CTB_CUDA_TRY(cudaMalloc(&t.K, sizeof(float) * t.M));
-    int st = ctb::filter_build_tables(W, pad, filter, t.M, t.tw, t.K, s);
-    if (st != CTB_OK) return st;
-    CTB_CUDA_TRY(cudaStreamSynchronize(s));
-    g_tables[key] = t;
-    *out = t;
-    return CTB_OK;
-}
 
 bool valid_detector(const ctb_detector* d) {
     return d && d->width > 1 && d->height > 1 && d->fcd > float(d->width) && d->base_intensity != 0.0f;
@@ -158,8 +114,8 @@ int ctb_filter_projections(const void* raw, int raw_type, int n_views, const ctb
     if (filter < CTB_RAMLAK || filter > CTB_HANN) return arg_error("unknown filter type");
     if (pad != 1 && pad != 2) return arg_error("pad must be 1 or 2");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    Tables t;
-    int st = get_tables(det->width, pad, filter, s, &t);
+    ctb::FilterTables t;
+    int st = ctb::filter_tables(det->width, pad, filter, s, &t);
     if (st != CTB_OK) return st;
     const ctb::FilterArgs a = ctb::filter_args(*det, raw_type, t.M, t.logM, n_views, store_scale);
     return ctb::filter_launch(raw, raw_type, filtered, store_type, a, t.tw, t.K, s);
@@ -263,6 +219,30 @@ int ctb_set_filter(ctb_ctx* ctx, int filter) { CTX_CHECK(ctx); return ctx->r.set
 int ctb_set_skip_projections(ctb_ctx* ctx, unsigned skip) { CTX_CHECK(ctx); return ctx->r.set_skip(skip); }
 int ctb_set_device(ctb_ctx* ctx, int device) { CTX_CHECK(ctx); return ctx->r.set_device(device); }
 int ctb_set_gpu_spare_memory(ctb_ctx* ctx, size_t mb) { CTX_CHECK(ctx); return ctx->r.set_spare_mb(mb); }
+int ctb_set_devices(ctb_ctx* ctx, const int* ids, int n) {
+    CTX_CHECK(ctx);
+    if (!ids || n <= 0) return arg_error("empty device list");
+    return ctx->r.set_devices(ids, n);
+}
+int ctb_set_gpu_coefficients(ctb_ctx* ctx, double mp, double bw) {
+    CTX_CHECK(ctx);
+    return ctx->r.set_gpu_coefficients(mp, bw);
+}
+int ctb_get_gpu_weights(ctb_ctx* ctx, const int* ids, int n, double* weights) {
+    CTX_CHECK(ctx);
+    if (!ids || !weights || n <= 0) return arg_error("empty device list");
+    return ctx->r.gpu_weights(ids, n, weights);
+}
+int ctb_gpu_weights_from(const int* sm_count, const double* bandwidth, int n, double mp, double bw, double* weights) {
+    if (!sm_count || !bandwidth || !weights || n <= 0) return arg_error("empty device list");
+    ctb::gpu_weights_from(sm_count, bandwidth, n, mp, bw, weights);
+    return CTB_OK;
+}
+int ctb_split_slices(const double* weights, int n, int z, int* begin) {
+    if (!weights || !begin || n <= 0 || z < 0) return arg_error("invalid split arguments");
+    ctb::split_slices(weights, n, z, begin);
+    return CTB_OK;
+}
 int ctb_set_precision(ctb_ctx* ctx, int store_type) { CTX_CHECK(ctx); return ctx->r.set_precision(store_type); }
 int ctb_set_pad(ctb_ctx* ctx, int pad) { CTX_CHECK(ctx); return ctx->r.set_pad(pad); }
 int ctb_set_grid(ctb_ctx* ctx, int x, int y, int z, float vs) { CTX_CHECK(ctx); return ctx->r.set_grid(x, y, z, vs); }
@@ -319,6 +299,14 @@ int ctb_save_volume(ctb_ctx* ctx, const char* path, int index_order, int byte_or
     CTX_CHECK(ctx);
     if (!path) return arg_error("null path");
     return ctx->r.save(path, index_order, byte_order);
+}
+
+int ctb_get_cross_section(const ctb_ctx* ctx, int axis, int index, float* out, int* rows, int* cols) {
+    CTX_CHECK(ctx);
+    if (axis < CTB_AXIS_X || axis > CTB_AXIS_Z) return arg_error("unknown axis");
+    const int st = ctx->r.cross_section(axis, index, out, rows, cols);
+    if (st != CTB_OK) ctb::set_global_error("no reconstructed volume or index out of bounds");
+    return st;
 }
 
 void ctb_stop(ctb_ctx* ctx) {

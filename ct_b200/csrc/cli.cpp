@@ -31,8 +31,10 @@ void usage() {
         "\t\t\t'hann'. Long: --filter. Default: ramlak\n"
         "\t-n \t\tOptional. Disables CUDA (not available: this engine reconstructs on the GPU). Long: --nocuda.\n"
         "\t-c \t\tOptional. CPU preprocessing (ignored: preprocessing runs on the GPU). Long: --cpuPreprocessing.\n"
-        "\t-d 0,1,..,n \tOptional. CUDA devices; the first one is used. Long: --cudadevices. Default: 0\n"
-        "\t-w x,y \t\tOptional. GPU weight coefficients (accepted for compatibility). Long: --weights.\n"
+        "\t-d 0,1,..,n \tOptional. CUDA devices; each reconstructs a share of the z slices.\n"
+        "\t\t\tLong: --cudadevices. Default: 0\n"
+        "\t-w x,y \t\tOptional. Exponents of the multiprocessor and memory-bandwidth shares in the\n"
+        "\t\t\tper-device weights. Long: --weights. Default: 1,1\n"
         "\t-m [number] \tOptional. VRAM to spare in Mb. Long: --cudasparememory. Default: 200\n"
         "\t-e [option] \tOptional. Byte order of the output, 'littleendian' or 'bigendian'. Long: --byteorder.\n"
         "\t-j [option] \tOptional. Index order of the output, 'zfastest' or 'xfastest'. Long: --indexorder.\n"
@@ -71,8 +73,10 @@ int main(int argc, char** argv) {
     }
     std::string input, output;
     bool have_in = false, have_out = false, nocuda = false;
-    int filter = CTB_RAMLAK, order = CTB_X_FASTEST, endian = CTB_LITTLE_ENDIAN, device = 0, store = CTB_FP32;
+    int filter = CTB_RAMLAK, order = CTB_X_FASTEST, endian = CTB_LITTLE_ENDIAN, store = CTB_FP32;
     int pad = 1, slab = 0;
+    std::vector<int> devices{0};
+    double mp_coef = 1, bw_coef = 1;
     double spare = 200, xmin = 0, xmax = 1, ymin = 0, ymax = 1, zmin = 0, zmax = 1;
     int gx = 0, gy = 0, gz = 0;
     double gvs = 1;
@@ -106,7 +110,14 @@ int main(int argc, char** argv) {
                     std::printf("When using the flag -d you have to specify at least one device ID.\n");
                     return 1;
                 }
-                device = std::atoi(list.substr(0, list.find(',')).c_str());
+                devices.clear();
+                size_t at = 0;
+                while (true) {
+                    const size_t comma = list.find(',', at);
+                    devices.push_back(std::atoi(list.substr(at, comma - at).c_str()));
+                    if (comma == std::string::npos) break;
+                    at = comma + 1;
+                }
             }
         } else if (a == "-m" || a == "--cudasparememory") {
             parse_double(argc, argv, ++i, &spare);
@@ -121,6 +132,8 @@ int main(int argc, char** argv) {
                     std::printf("When using the flag -w you have to specify exactly two coefficients.\n");
                     return 1;
                 }
+                mp_coef = std::strtod(w.c_str(), nullptr);
+                bw_coef = std::strtod(w.c_str() + w.find(',') + 1, nullptr);
             }
         } else if (a == "--precision") {
             if (++i < argc) {
@@ -159,7 +172,9 @@ int main(int argc, char** argv) {
         return 1;
     };
     ctb_set_progress_callback(ctx, progress, nullptr);
-    if (ctb_set_device(ctx, device) != CTB_OK) return fail("device");
+    if (ctb_set_devices(ctx, devices.data(), int(devices.size())) != CTB_OK)
+        std::printf("%s\n", ctb_last_error(ctx));  // the previous selection stays, as in the reference
+    ctb_set_gpu_coefficients(ctx, mp_coef, bw_coef);
     ctb_set_gpu_spare_memory(ctx, size_t(spare));
     ctb_set_precision(ctx, store);
     if (ctb_set_pad(ctx, pad) != CTB_OK) return fail("pad");

@@ -5,6 +5,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #include "../../include/ctb.h"
 
@@ -44,12 +45,22 @@ int filter_transform_length(int W, int pad);
 // tw and K must hold M entries each. Stream-ordered.
 int filter_build_tables(int W, int pad, int filter, int M, float2* tw, float* K, cudaStream_t s);
 
+// Device tables of a (W, pad, filter) triple on the current device, built on
+// first use and kept for the life of the process.
+struct FilterTables {
+    int M = 0, logM = 0;
+    const float2* tw = nullptr;
+    const float* K = nullptr;
+};
+int filter_tables(int W, int pad, int filter, cudaStream_t s, FilterTables* out);
+
 struct FilterArgs {
     int W, H, M, logM;
     long long n_views;
     float alpha, beta, log_scale;   // convertTo alpha/beta and the log pre-scale
     float D, uPre, vPre;            // Feldkamp weight
     float store_scale;
+    int out_pitch;                  // elements per filtered row (>= W; padding is left untouched)
 };
 
 // Launch the fused load/log/weight/FFT/window/IFFT/store kernel over n_views.
@@ -80,7 +91,8 @@ struct ProjGeom {
                                 // voxel's row coordinate does not depend on the slabbing
     float vi_hi;                // largest valid row coordinate: float(H - 1.1)
     float load_scale;
-    long long view_stride;      // elements between consecutive projections
+    int pitch;                  // elements per projection row (>= W)
+    long long view_stride;      // elements between consecutive projections (H * pitch)
 };
 
 ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_end, float load_scale);
@@ -93,9 +105,38 @@ int backproject_launch(const void* proj, int store_type, const float4* views, in
 int backproject_global_launch(const void* proj, int store_type, const float4* views, int n_views,
                               const ProjGeom& g, float* vol, int accumulate, cudaStream_t s);
 // Returns CTB_ERR_UNSUPPORTED (nothing launched) when the geometry or layout
-// does not suit the TMA kernel.
+// does not suit the TMA kernel. zc: z voxels per thread (8 or 16).
 int backproject_tma_launch(const void* proj, int store_type, const float4* views, int n_views,
-                           const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s);
+                           const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s,
+                           int zc = 16);
+
+// Persistent multi-scan backprojection: one launch takes (scan, tile) work
+// items from a device counter until every scan of the batch is done.
+struct BpBatchScan {
+    const void* proj;       // filtered projections (row pitch g.pitch)
+    const float4* views;    // device view table
+    int n_views;
+    ProjGeom g;
+    double hmax;
+    float* vol;             // X-fastest slab of the box
+    int accumulate;
+};
+struct BpBatchPlan {
+    int store_type = 0, zc = 16, nbuf = 3, buf_stride = 0, grid = 0;
+    size_t smem = 0, desc_size = 0;
+    long long total_tiles = 0;
+    std::vector<unsigned char> desc;   // descriptors of the included scans (host copy, to be uploaded)
+    std::vector<long long> tile_start; // included + 1 prefix sums of tiles
+    std::vector<int> included;         // scans handled by the persistent kernel
+    std::vector<int> excluded;         // scans whose footprint does not suit it (global-gather kernel)
+};
+// Builds descriptors (tensor maps, boxes, tile counts) and launch shape for
+// every scan that suits the shared-memory kernel; lists the others.
+int bp_batch_plan(int store_type, int zc, const BpBatchScan* scans, int n, BpBatchPlan* plan);
+// desc / tile_start: device copies of plan.desc / plan.tile_start; queue: a
+// device counter that must be zero at launch.
+int bp_batch_launch(const BpBatchPlan& plan, const void* desc, const long long* tile_start, int n,
+                    unsigned long long* queue, cudaStream_t s);
 // Number of CTAs whose bounded mbarrier waits gave up since the last reset.
 int device_wait_timeouts(unsigned* count, int reset);
 

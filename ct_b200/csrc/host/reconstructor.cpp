@@ -146,16 +146,43 @@ unsigned cylinder_radius(int W, float FCD) {
 
 }  // namespace
 
+DeviceWork::~DeviceWork() {
+    // device buffers belong to this worker's device
+    cudaSetDevice(device);
+    if (s_copy) {
+        cudaStreamDestroy(s_copy);
+        cudaStreamDestroy(s_comp);
+        cudaStreamDestroy(s_down);
+    }
+    for (DevBuf* b : {&d_filtered, &d_ring, &d_views, &d_angles, &d_heights, &d_tw, &d_K, &d_slab[0], &d_slab[1],
+                      &d_conv[0], &d_conv[1]})
+        b->release();
+}
+
+void gpu_weights_from(const int* sm_count, const double* bandwidth, int n, double mp_coef, double bw_coef,
+                      double* weights) {
+    double sm_total = 0, bw_total = 0;
+    for (int i = 0; i < n; ++i) { sm_total += sm_count[i]; bw_total += bandwidth[i]; }
+    double sum = 0;
+    for (int i = 0; i < n; ++i) {
+        weights[i] = std::pow(double(sm_count[i]) / sm_total, mp_coef) * std::pow(bandwidth[i] / bw_total, bw_coef);
+        sum += weights[i];
+    }
+    for (int i = 0; i < n; ++i) weights[i] /= sum;
+}
+
+void split_slices(const double* weights, int n, int z, int* begin) {
+    int cur = 0;
+    for (int i = 0; i < n; ++i) {
+        begin[i] = cur;
+        cur = std::min(z, cur + int(std::lround(weights[i] * double(z))));
+    }
+    begin[n] = z;
+}
+
 Reconstructor::Reconstructor() {}
 
-Reconstructor::~Reconstructor() {
-    if (s_copy_) {
-        cudaSetDevice(device_);
-        cudaStreamDestroy(s_copy_);
-        cudaStreamDestroy(s_comp_);
-        cudaStreamDestroy(s_down_);
-    }
-}
+Reconstructor::~Reconstructor() {}
 
 int Reconstructor::fail(int status, const std::string& msg) {
     err_ = msg;
@@ -210,17 +237,43 @@ int Reconstructor::set_device(int d) {
         cudaGetLastError();
         return fail(CTB_ERR_ARG, "Active CUDA device was not set because the device ID is not valid.");
     }
-    if (s_copy_ && d != device_) {
-        cudaSetDevice(device_);
-        cudaStreamDestroy(s_copy_); cudaStreamDestroy(s_comp_); cudaStreamDestroy(s_down_);
-        s_copy_ = s_comp_ = s_down_ = nullptr;
-        d_filtered_.release(); d_ring_.release(); d_views_.release(); d_angles_.release();
-        d_heights_.release(); d_tw_.release(); d_K_.release();
-        for (auto& b : d_slab_) b.release();
-        for (auto& b : d_conv_) b.release();
-        tables_key_[0] = -1;
+    devices_.assign(1, d);
+    return CTB_OK;
+}
+
+// setActiveCudaDevices (Ct/CtVolume.cpp:506-520): IDs beyond the device count
+// are dropped; with none left the previous selection stays. A device may be
+// listed more than once: each entry is its own worker with its own buffers.
+int Reconstructor::set_devices(const int* ids, int n) {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess) {
+        cudaGetLastError();
+        count = 0;
     }
-    device_ = d;
+    std::vector<int> keep;
+    for (int i = 0; i < n; ++i)
+        if (ids[i] >= 0 && ids[i] < count) keep.push_back(ids[i]);
+    if (keep.empty())
+        return fail(CTB_ERR_ARG, "Active CUDA devices were not set because vector did not contain any valid device ID.");
+    devices_ = keep;
+    return CTB_OK;
+}
+
+int Reconstructor::gpu_weights(const int* ids, int n, double* weights) {
+    std::vector<int> sm(n);
+    std::vector<double> bw(n);
+    for (int i = 0; i < n; ++i) {
+        int s = 0, bus = 0, clk = 0;
+        if (cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, ids[i]) != cudaSuccess ||
+            cudaDeviceGetAttribute(&bus, cudaDevAttrGlobalMemoryBusWidth, ids[i]) != cudaSuccess ||
+            cudaDeviceGetAttribute(&clk, cudaDevAttrMemoryClockRate, ids[i]) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(CTB_ERR_ARG, "device properties could not be queried");
+        }
+        sm[i] = s;
+        bw[i] = double(bus) * double(clk);
+    }
+    gpu_weights_from(sm.data(), bw.data(), n, mp_coef_, bw_coef_, weights);
     return CTB_OK;
 }
 
@@ -425,6 +478,7 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
                                  "load some images first.");
     const int X = grid_.x_to - grid_.x_from, Y = grid_.y_to - grid_.y_from, Z = grid_.z_to - grid_.z_from;
     if (X <= 0 || Y <= 0 || Z <= 0) return fail(CTB_ERR_ARG, "The reconstructed box is empty.");
+    const auto t_start = std::chrono::steady_clock::now();
     float* target = host_out;
     if (!target) {
         if (volume_.ensure(sizeof(float) * size_t(X) * Y * Z) != CTB_OK)
@@ -433,31 +487,100 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
         target = static_cast<float*>(volume_.p);
         index_order = CTB_X_FASTEST;
     }
-    const int st = run_pipeline(target, index_order);
-    if (st != CTB_OK) {
+
+    // one worker per active device entry; workers keep their buffers while
+    // the device list stays the same
+    const int n = int(devices_.size());
+    for (int i = 0; i < n; ++i)
+        if (i >= int(workers_.size()) || workers_[i]->device != devices_[i]) {
+            if (i < int(workers_.size())) workers_[i].reset(new DeviceWork(devices_[i]));
+            else workers_.emplace_back(new DeviceWork(devices_[i]));
+        }
+    workers_.resize(n);
+    std::vector<double> weights(n, 1.0);
+    if (n > 1 && gpu_weights(devices_.data(), n, weights.data()) != CTB_OK) return CTB_ERR_ARG;
+    std::vector<int> begin(n + 1);
+    split_slices(weights.data(), n, Z, begin.data());
+    for (int i = 0; i < n; ++i) {
+        workers_[i]->progress = 0;
+        workers_[i]->share = double(begin[i + 1] - begin[i]) / double(Z);
+    }
+
+    std::vector<int> st(n, CTB_OK);
+    auto work = [&](int i) {
+        st[i] = run_pipeline(*workers_[i], target, index_order, begin[i], begin[i + 1]);
+        if (st[i] != CTB_OK && st[i] != CTB_INTERRUPTED) stop_ = true;  // the other workers end early
+    };
+    if (n == 1) {
+        work(0);
+    } else {
+        std::vector<std::thread> threads;
+        for (int i = 0; i < n; ++i) threads.emplace_back(work, i);
+        for (auto& t : threads) t.join();
+    }
+    int status = CTB_OK;
+    std::string msg;
+    for (int i = 0; i < n; ++i)
+        if (st[i] != CTB_OK && (status == CTB_OK || status == CTB_INTERRUPTED)) {
+            status = st[i];
+            msg = workers_[i]->err;
+        }
+    if (status != CTB_OK) {
         if (!host_out) vol_dims_[0] = vol_dims_[1] = vol_dims_[2] = 0;  // volume.clear() (:617)
-        return st;
+        return fail(status, msg);
     }
     if (!host_out) { vol_dims_[0] = X; vol_dims_[1] = Y; vol_dims_[2] = Z; }
+
+    ctb_timings t{};
+    for (auto& w : workers_) {
+        t.filter_s = std::max(t.filter_s, w->filter_s);
+        t.backproject_s = std::max(t.backproject_s, w->backproject_s);
+        t.upload_s = std::max(t.upload_s, w->upload_s);
+        t.download_s = std::max(t.download_s, w->download_s);
+    }
+    t.total_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    const int step = std::max(1, step_);
+    t.voxel_views = double(X) * Y * Z * double((int(angles_.size()) + step - 1) / step);
+    tm_ = t;
     return CTB_OK;
 }
 
-int Reconstructor::run_pipeline(float* out, int order) {
+// emitGlobalCudaProgress (Ct/CtVolume.cpp:1469-1485): the total is each
+// worker's completion weighted by its share of the slices.
+void Reconstructor::worker_progress(DeviceWork& w, double frac) {
+    std::lock_guard<std::mutex> lk(progress_mtx_);
+    w.progress = frac;
+    double total = 0;
+    for (auto& o : workers_) total += o->progress * o->share;
+    progress(1, 100.0 * total);
+}
+
+// Reconstructs box slices [z_lo, z_hi) on worker w's device into out, which
+// holds the whole box in the requested index order (cudaReconstructionCore,
+// Ct/CtVolume.cpp:1155-1320, for one device's part of the volume).
+int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, int z_hi) {
     const auto t_start = std::chrono::steady_clock::now();
-    if (cudaSetDevice(device_) != cudaSuccess) {
+    auto fail = [&w](int status, const std::string& msg) {
+        w.err = msg;
+        return status;
+    };
+    w.filter_s = w.backproject_s = w.upload_s = w.download_s = 0;
+    if (z_hi <= z_lo) return CTB_OK;
+    if (cudaSetDevice(w.device) != cudaSuccess) {
         cudaGetLastError();
         return fail(CTB_ERR_CUDA, "CUDA device could not be selected.");
     }
-    if (!s_copy_) {
-        if (cudaStreamCreateWithFlags(&s_copy_, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaStreamCreateWithFlags(&s_comp_, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaStreamCreateWithFlags(&s_down_, cudaStreamNonBlocking) != cudaSuccess) {
+    if (!w.s_copy) {
+        if (cudaStreamCreateWithFlags(&w.s_copy, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&w.s_comp, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&w.s_down, cudaStreamNonBlocking) != cudaSuccess) {
             cudaGetLastError();
             return fail(CTB_ERR_CUDA, "CUDA streams could not be created.");
         }
     }
     const int W = det_.width, H = det_.height;
     const int X = grid_.x_to - grid_.x_from, Y = grid_.y_to - grid_.y_from, Z = grid_.z_to - grid_.z_from;
+    const int Zw = z_hi - z_lo;  // this worker's slices
 
     // views used (setSkipProjections: projectionStep, :945)
     std::vector<int> used;
@@ -482,11 +605,14 @@ int Reconstructor::run_pipeline(float* out, int order) {
 
     // ---- sizing
     const size_t view_raw = size_t(W) * H * raw_bytes(raw_type_);
-    const size_t view_filt = size_t(W) * H * store_bytes(store_);
+    // filtered rows padded to a 16-byte multiple so every width can use the
+    // shared-memory (TMA) backprojector
+    const int pitch = (W + 7) / 8 * 8;
+    const size_t view_filt = size_t(pitch) * H * store_bytes(store_);
     const int chunk = int(std::max<size_t>(1, std::min<size_t>(size_t(V), (size_t(256) << 20) / view_raw)));
     const size_t plane = size_t(X) * Y;
-    int slab = slab_req_ > 0 ? slab_req_ : std::max(16, ((Z + 7) / 8 + 15) / 16 * 16);
-    slab = std::min(slab, Z);
+    int slab = slab_req_ > 0 ? slab_req_ : std::max(16, ((Zw + 7) / 8 + 15) / 16 * 16);
+    slab = std::min(slab, Zw);
     const bool convert = order == CTB_Z_FASTEST;
     {
         size_t freeb = 0, total = 0;
@@ -496,7 +622,7 @@ int Reconstructor::run_pipeline(float* out, int order) {
             return view_filt * V + 3 * view_raw * chunk + 2 * plane * sl * 4 * (convert ? 2 : 1) + 64 * V +
                    size_t(M) * 12;
         };
-        const size_t have = d_filtered_.bytes + d_ring_.bytes + d_slab_[0].bytes * 2 + d_conv_[0].bytes * 2;
+        const size_t have = w.d_filtered.bytes + w.d_ring.bytes + w.d_slab[0].bytes * 2 + w.d_conv[0].bytes * 2;
         while (slab > 16 && need(slab) > freeb + have - std::min(freeb + have, spare)) slab = std::max(16, slab / 2);
         if (need(slab) + spare > freeb + have)
             return fail(CTB_ERR_ALLOC,
@@ -504,29 +630,29 @@ int Reconstructor::run_pipeline(float* out, int order) {
                         "of free VRAM was insufficient. You can try changing the GPU spare memory setting.");
     }
     int st;
-    if ((st = d_filtered_.ensure(view_filt * V, "filtered projections")) ||
-        (st = d_ring_.ensure(3 * view_raw * chunk, "projection upload ring")) ||
-        (st = d_views_.ensure(sizeof(float4) * V, "view table")) ||
-        (st = d_angles_.ensure(sizeof(double) * V, "angles")) ||
-        (st = d_heights_.ensure(sizeof(double) * V, "height offsets")) ||
-        (st = d_tw_.ensure(sizeof(float2) * M, "twiddles")) || (st = d_K_.ensure(sizeof(float) * M, "filter")))
+    if ((st = w.d_filtered.ensure(view_filt * V, "filtered projections")) ||
+        (st = w.d_ring.ensure(3 * view_raw * chunk, "projection upload ring")) ||
+        (st = w.d_views.ensure(sizeof(float4) * V, "view table")) ||
+        (st = w.d_angles.ensure(sizeof(double) * V, "angles")) ||
+        (st = w.d_heights.ensure(sizeof(double) * V, "height offsets")) ||
+        (st = w.d_tw.ensure(sizeof(float2) * M, "twiddles")) || (st = w.d_K.ensure(sizeof(float) * M, "filter")))
         return fail(st, global_error());
     for (int b = 0; b < 2; ++b) {
-        if ((st = d_slab_[b].ensure(sizeof(float) * plane * slab, "volume slab"))) return fail(st, global_error());
-        if (convert && (st = d_conv_[b].ensure(sizeof(float) * plane * slab, "layout slab")))
+        if ((st = w.d_slab[b].ensure(sizeof(float) * plane * slab, "volume slab"))) return fail(st, global_error());
+        if (convert && (st = w.d_conv[b].ensure(sizeof(float) * plane * slab, "layout slab")))
             return fail(st, global_error());
     }
     const bool out_pinned = is_pinned(out);
     if (!out_pinned)
-        for (auto& hb : h_stage_)
+        for (auto& hb : w.h_stage)
             if (hb.ensure(sizeof(float) * plane * slab) != CTB_OK || !hb.pinned)
                 return fail(CTB_ERR_ALLOC, "Pinned staging memory could not be allocated.");
 
     // ---- events
     cudaEvent_t ev_up[3], ev_free[3], ev_bp[2], ev_down[2], e_f0, e_f1, e_b0, e_b1;
     const int nchunks = (V + chunk - 1) / chunk;
-    const int nslabs = (Z + slab - 1) / slab;
-    std::vector<cudaEvent_t> tf(2 * nchunks), tb(2 * nslabs);
+    const int nslabs = (Zw + slab - 1) / slab;
+    std::vector<cudaEvent_t> tf(2 * nchunks), tb(2 * (nslabs + nchunks));
     for (auto& e : tf) cudaEventCreate(&e);
     for (auto& e : tb) cudaEventCreate(&e);
     for (auto& e : ev_up) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
@@ -544,66 +670,82 @@ int Reconstructor::run_pipeline(float* out, int order) {
         for (auto& e : tb) cudaEventDestroy(e);
     };
     auto cuda_fail = [&](const char* what) {
-        cudaStreamSynchronize(s_copy_); cudaStreamSynchronize(s_comp_); cudaStreamSynchronize(s_down_);
+        cudaStreamSynchronize(w.s_copy); cudaStreamSynchronize(w.s_comp); cudaStreamSynchronize(w.s_down);
         cleanup();
         const cudaError_t e = cudaGetLastError();
         return fail(CTB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     };
 
     // ---- geometry tables (FP64 kernels)
-    if (cudaMemcpyAsync(d_angles_.p, ang.data(), sizeof(double) * V, cudaMemcpyHostToDevice, s_comp_) ||
-        cudaMemcpyAsync(d_heights_.p, hp.data(), sizeof(double) * V, cudaMemcpyHostToDevice, s_comp_))
+    if (cudaMemcpyAsync(w.d_angles.p, ang.data(), sizeof(double) * V, cudaMemcpyHostToDevice, w.s_comp) ||
+        cudaMemcpyAsync(w.d_heights.p, hp.data(), sizeof(double) * V, cudaMemcpyHostToDevice, w.s_comp))
         return cuda_fail("geometry upload");
-    if (view_table_build((double*)d_angles_.p, (double*)d_heights_.p, V, (float4*)d_views_.p, s_comp_))
+    if (view_table_build((double*)w.d_angles.p, (double*)w.d_heights.p, V, (float4*)w.d_views.p, w.s_comp))
         return cuda_fail("view table");
-    if (tables_key_[0] != W || tables_key_[1] != pad_ || tables_key_[2] != filter_) {
-        if (filter_build_tables(W, pad_, filter_, M, (float2*)d_tw_.p, (float*)d_K_.p, s_comp_))
+    if (w.tables_key[0] != W || w.tables_key[1] != pad_ || w.tables_key[2] != filter_) {
+        if (filter_build_tables(W, pad_, filter_, M, (float2*)w.d_tw.p, (float*)w.d_K.p, w.s_comp))
             return cuda_fail("filter tables");
-        tables_key_[0] = W; tables_key_[1] = pad_; tables_key_[2] = filter_;
+        w.tables_key[0] = W; w.tables_key[1] = pad_; w.tables_key[2] = filter_;
     }
     // the ring slots start free
-    for (auto& e : ev_free) cudaEventRecord(e, s_comp_);
+    for (auto& e : ev_free) cudaEventRecord(e, w.s_comp);
 
-    // ---- upload + filter
+    // ---- upload + filter; slab 0 is backprojected chunk by chunk as the views
+    // arrive, so the host-to-device transfer overlaps with its backprojection
     const bool in_pinned = is_pinned(images_);
-    cudaEventRecord(e_f0, s_comp_);
+    auto slab_geom = [&](int zb, int ze) {
+        ProjGeom g = proj_geom(det_, grid_, zb, ze, load_scale);
+        g.pitch = pitch;
+        g.view_stride = (long long)pitch * H;
+        return g;
+    };
+    const ProjGeom g0 = slab_geom(z_lo, std::min(z_hi, z_lo + slab));
+    int nb_ev = 0;  // backprojection event pairs used
+    cudaEventRecord(e_f0, w.s_comp);
     int slot = 0;
     for (int c0 = 0; c0 < V; c0 += chunk, slot = (slot + 1) % 3) {
         if (stop_) { cuda_fail("stop"); return fail(CTB_INTERRUPTED, "User interrupted. Stopping."); }
         const int n = std::min(chunk, V - c0);
-        char* dst = (char*)d_ring_.p + size_t(slot) * view_raw * chunk;
-        cudaStreamWaitEvent(s_copy_, ev_free[slot], 0);
+        char* dst = (char*)w.d_ring.p + size_t(slot) * view_raw * chunk;
+        cudaStreamWaitEvent(w.s_copy, ev_free[slot], 0);
         if (step_ <= 1) {
             if (cudaMemcpyAsync(dst, (const char*)images_ + size_t(c0) * view_raw, view_raw * n,
-                                cudaMemcpyHostToDevice, s_copy_))
+                                cudaMemcpyHostToDevice, w.s_copy))
                 return cuda_fail("projection upload");
         } else {
             for (int i = 0; i < n; ++i)
                 if (cudaMemcpyAsync(dst + size_t(i) * view_raw, (const char*)images_ + size_t(used[c0 + i]) * view_raw,
-                                    view_raw, cudaMemcpyHostToDevice, s_copy_))
+                                    view_raw, cudaMemcpyHostToDevice, w.s_copy))
                     return cuda_fail("projection upload");
         }
-        cudaEventRecord(ev_up[slot], s_copy_);
-        cudaStreamWaitEvent(s_comp_, ev_up[slot], 0);
-        const FilterArgs fa = filter_args(det_, raw_type_, M, logM, n, store_scale);
-        cudaEventRecord(tf[2 * (c0 / chunk)], s_comp_);
-        if (filter_launch(dst, raw_type_, (char*)d_filtered_.p + size_t(c0) * view_filt, store_, fa,
-                          (const float2*)d_tw_.p, (const float*)d_K_.p, s_comp_))
+        cudaEventRecord(ev_up[slot], w.s_copy);
+        cudaStreamWaitEvent(w.s_comp, ev_up[slot], 0);
+        FilterArgs fa = filter_args(det_, raw_type_, M, logM, n, store_scale);
+        fa.out_pitch = pitch;
+        cudaEventRecord(tf[2 * (c0 / chunk)], w.s_comp);
+        char* fdst = (char*)w.d_filtered.p + size_t(c0) * view_filt;
+        if (filter_launch(dst, raw_type_, fdst, store_, fa, (const float2*)w.d_tw.p, (const float*)w.d_K.p, w.s_comp))
             return cuda_fail("filter launch");
-        cudaEventRecord(tf[2 * (c0 / chunk) + 1], s_comp_);
-        cudaEventRecord(ev_free[slot], s_comp_);
-        if (!in_pinned) cudaStreamSynchronize(s_copy_);
+        cudaEventRecord(tf[2 * (c0 / chunk) + 1], w.s_comp);
+        cudaEventRecord(ev_free[slot], w.s_comp);
+        cudaEventRecord(tb[2 * nb_ev], w.s_comp);
+        if (backproject_launch(fdst, store_, (const float4*)w.d_views.p + c0, n, g0, hmax, (float*)w.d_slab[0].p,
+                               c0 > 0, w.s_comp))
+            return cuda_fail("backprojection launch");
+        cudaEventRecord(tb[2 * nb_ev + 1], w.s_comp);
+        ++nb_ev;
+        if (!in_pinned) cudaStreamSynchronize(w.s_copy);
     }
-    cudaEventRecord(e_f1, s_comp_);
+    cudaEventRecord(e_f1, w.s_comp);
 
     // ---- backprojection per slab + layout + download
-    cudaEventRecord(e_b0, s_comp_);
+    cudaEventRecord(e_b0, w.s_comp);
     auto host_copy = [&](int k) {
         // pageable output: staged slab k -> final position
         const int b = k % 2;
-        const int zb = k * slab, zs = std::min(slab, Z - zb);
+        const int zb = z_lo + k * slab, zs = std::min(slab, z_hi - zb);
         cudaEventSynchronize(ev_down[b]);
-        const float* src = (const float*)h_stage_[b].p;
+        const float* src = (const float*)w.h_stage[b].p;
         if (order == CTB_Z_FASTEST) {
             parallel_for(plane, [&](size_t i) {
                 std::memcpy(out + i * Z + zb, src + i * zs, sizeof(float) * zs);
@@ -620,58 +762,65 @@ int Reconstructor::run_pipeline(float* out, int order) {
     for (int k = 0; k < nslabs; ++k) {
         if (stop_) { cuda_fail("stop"); return fail(CTB_INTERRUPTED, "User interrupted. Stopping."); }
         const int b = k % 2;
-        const int zb = k * slab, ze = std::min(Z, zb + slab), zs = ze - zb;
-        if (k >= 2) cudaStreamWaitEvent(s_comp_, ev_down[b], 0);
-        const ProjGeom g = proj_geom(det_, grid_, zb, ze, load_scale);
-        cudaEventRecord(tb[2 * k], s_comp_);
-        if (backproject_launch(d_filtered_.p, store_, (const float4*)d_views_.p, V, g, hmax, (float*)d_slab_[b].p, 0,
-                               s_comp_))
-            return cuda_fail("backprojection launch");
-        cudaEventRecord(tb[2 * k + 1], s_comp_);
-        const float* src = (const float*)d_slab_[b].p;
-        if (convert) {
-            if (layout_launch(src, X, Y, zs, CTB_Z_FASTEST, CTB_LITTLE_ENDIAN, d_conv_[b].p, s_comp_))
-                return cuda_fail("layout launch");
-            src = (const float*)d_conv_[b].p;
+        const int zb = z_lo + k * slab, ze = std::min(z_hi, zb + slab), zs = ze - zb;
+        if (k >= 2) cudaStreamWaitEvent(w.s_comp, ev_down[b], 0);
+        if (k > 0) {  // slab 0 was backprojected during the upload
+            const ProjGeom g = slab_geom(zb, ze);
+            cudaEventRecord(tb[2 * nb_ev], w.s_comp);
+            if (backproject_launch(w.d_filtered.p, store_, (const float4*)w.d_views.p, V, g, hmax,
+                                   (float*)w.d_slab[b].p, 0, w.s_comp))
+                return cuda_fail("backprojection launch");
+            cudaEventRecord(tb[2 * nb_ev + 1], w.s_comp);
+            ++nb_ev;
         }
-        cudaEventRecord(ev_bp[b], s_comp_);
-        cudaStreamWaitEvent(s_down_, ev_bp[b], 0);
+        const float* src = (const float*)w.d_slab[b].p;
+        if (convert) {
+            if (layout_launch(src, X, Y, zs, CTB_Z_FASTEST, CTB_LITTLE_ENDIAN, w.d_conv[b].p, w.s_comp))
+                return cuda_fail("layout launch");
+            src = (const float*)w.d_conv[b].p;
+        }
+        cudaEventRecord(ev_bp[b], w.s_comp);
+        cudaStreamWaitEvent(w.s_down, ev_bp[b], 0);
         cudaError_t ce;
         if (out_pinned) {
             if (convert)
                 ce = cudaMemcpy2DAsync(out + zb, sizeof(float) * Z, src, sizeof(float) * zs, sizeof(float) * zs,
-                                       plane, cudaMemcpyDeviceToHost, s_down_);
+                                       plane, cudaMemcpyDeviceToHost, w.s_down);
             else
                 ce = cudaMemcpyAsync(out + size_t(zb) * plane, src, sizeof(float) * plane * zs,
-                                     cudaMemcpyDeviceToHost, s_down_);
+                                     cudaMemcpyDeviceToHost, w.s_down);
         } else {
             if (k >= 2) host_copy(k - 2);  // frees staging buffer b
-            ce = cudaMemcpyAsync(h_stage_[b].p, src, sizeof(float) * plane * zs, cudaMemcpyDeviceToHost, s_down_);
+            ce = cudaMemcpyAsync(w.h_stage[b].p, src, sizeof(float) * plane * zs, cudaMemcpyDeviceToHost, w.s_down);
         }
         if (ce != cudaSuccess) return cuda_fail("volume download");
-        cudaEventRecord(ev_down[b], s_down_);
-        progress(1, 100.0 * double(k + 1) / double(nslabs));
+        cudaEventRecord(ev_down[b], w.s_down);
+        worker_progress(w, double(k + 1) / double(nslabs));
     }
-    cudaEventRecord(e_b1, s_comp_);
+    cudaEventRecord(e_b1, w.s_comp);
     if (!out_pinned)
         for (int k = std::max(0, nslabs - 2); k < nslabs; ++k) host_copy(k);
-    if (cudaStreamSynchronize(s_down_) != cudaSuccess || cudaStreamSynchronize(s_comp_) != cudaSuccess ||
-        cudaStreamSynchronize(s_copy_) != cudaSuccess)
+    if (cudaStreamSynchronize(w.s_down) != cudaSuccess || cudaStreamSynchronize(w.s_comp) != cudaSuccess ||
+        cudaStreamSynchronize(w.s_copy) != cudaSuccess)
         return cuda_fail("reconstruction");
     float phase_ms = 0, tail_ms = 0;
     double f_ms = 0, b_ms = 0;
     cudaEventElapsedTime(&phase_ms, e_f0, e_f1);
     for (int i = 0; i < nchunks; ++i) { float t = 0; cudaEventElapsedTime(&t, tf[2 * i], tf[2 * i + 1]); f_ms += t; }
-    for (int i = 0; i < nslabs; ++i) { float t = 0; cudaEventElapsedTime(&t, tb[2 * i], tb[2 * i + 1]); b_ms += t; }
+    double bp0_ms = 0;
+    for (int i = 0; i < nb_ev; ++i) {
+        float t = 0;
+        cudaEventElapsedTime(&t, tb[2 * i], tb[2 * i + 1]);
+        b_ms += t;
+        if (i < nchunks) bp0_ms += t;
+    }
     cudaEventElapsedTime(&tail_ms, e_b0, e_b1);
     cleanup();
     const double total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
-    tm_.filter_s = f_ms * 1e-3;
-    tm_.backproject_s = b_ms * 1e-3;
-    tm_.upload_s = std::max(0.0, (phase_ms - f_ms) * 1e-3);
-    tm_.download_s = std::max(0.0, total - (phase_ms + tail_ms) * 1e-3);
-    tm_.total_s = total;
-    tm_.voxel_views = double(X) * Y * Z * V;
+    w.filter_s = f_ms * 1e-3;
+    w.backproject_s = b_ms * 1e-3;
+    w.upload_s = std::max(0.0, (phase_ms - f_ms - bp0_ms) * 1e-3);
+    w.download_s = std::max(0.0, total - (phase_ms + tail_ms) * 1e-3);
     return CTB_OK;
 }
 

@@ -1,9 +1,12 @@
 // Reconstruction facade: the B200 counterpart of ct::CtVolume
-// (Ct/CtVolume.h:57-278). One context drives one device.
+// (Ct/CtVolume.h:57-278). One context drives one or more devices; each active
+// device reconstructs its own run of z slices from all views, as the
+// reference's launchCudaThreads does (Ct/CtVolume.cpp:1322-1351).
 #pragma once
 
 #include <atomic>
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -31,6 +34,32 @@ struct HostBuf {
     ~HostBuf() { release(); }
 };
 
+// Per-device resources of one reconstruction worker (one host thread per
+// active device). Buffers only grow and are reused across reconstructions.
+struct DeviceWork {
+    int device = 0;
+    cudaStream_t s_copy = nullptr, s_comp = nullptr, s_down = nullptr;
+    DevBuf d_filtered, d_ring, d_views, d_angles, d_heights, d_tw, d_K, d_slab[2], d_conv[2];
+    HostBuf h_stage[2];
+    int tables_key[3] = {-1, -1, -1};  // W, pad, filter of the cached tables
+    // outcome of the last run
+    std::string err;
+    double filter_s = 0, backproject_s = 0, upload_s = 0, download_s = 0;
+    double progress = 0;  // 0..1 of this worker's slices
+    double share = 1;     // this worker's fraction of all slices
+    explicit DeviceWork(int d) : device(d) {}
+    ~DeviceWork();
+};
+
+// getGpuWeights (Ct/CtVolume.cpp:1353-1381): per device
+// (sm_i / sum sm)^mp_coef * (bw_i / sum bw)^bw_coef, normalised to sum 1.
+void gpu_weights_from(const int* sm_count, const double* bandwidth, int n, double mp_coef, double bw_coef,
+                      double* weights);
+// Consecutive z ranges [begin[i], begin[i+1]) of round(weight_i * z) slices
+// (launchCudaThreads, Ct/CtVolume.cpp:1339-1344), clamped to z; the last
+// device also takes what rounding left over, so every slice is covered once.
+void split_slices(const double* weights, int n, int z, int* begin);
+
 class Reconstructor {
    public:
     Reconstructor();
@@ -47,6 +76,9 @@ class Reconstructor {
     int set_filter(int f);
     int set_skip(unsigned skip) { step_ = int(skip) + 1; return CTB_OK; }
     int set_device(int d);
+    int set_devices(const int* ids, int n);
+    int set_gpu_coefficients(double mp, double bw) { mp_coef_ = mp; bw_coef_ = bw; return CTB_OK; }
+    int gpu_weights(const int* ids, int n, double* weights);
     int set_spare_mb(size_t mb) { spare_mb_ = mb; return CTB_OK; }
     int set_precision(int t);
     int set_pad(int p);
@@ -64,6 +96,7 @@ class Reconstructor {
     // ---- work
     int reconstruct(float* host_out, int index_order);   // host_out == nullptr: keep internally
     int get_volume(float* host_out, int index_order) const;
+    int cross_section(int axis, int index, float* out, int* rows, int* cols) const;
     int save(const std::string& path, int index_order, int byte_order);
     void stop() { stop_ = true; }
 
@@ -75,8 +108,9 @@ class Reconstructor {
                     const double* angles_deg, const double* heights_mm, double pixel_size, int ccw,
                     double u_offset_mm, double fcd_mm, double base_intensity);
     void update_grid();
-    int run_pipeline(float* host_out, int index_order);
+    int run_pipeline(DeviceWork& w, float* host_out, int index_order, int z_lo, int z_hi);
     void progress(int stage, double pct) { if (cb_) cb_(stage, pct, cb_user_); }
+    void worker_progress(DeviceWork& w, double frac);
 
     std::mutex mtx_;                 // exclusiveFunctionsMutex (Ct/CtVolume.h:258)
     std::atomic<bool> stop_{false};  // stopActiveProcess (:245)
@@ -95,7 +129,8 @@ class Reconstructor {
     // settings
     int filter_ = CTB_RAMLAK;
     int step_ = 1;
-    int device_ = 0;
+    std::vector<int> devices_{0};    // activeCudaDevices (:241)
+    double mp_coef_ = 1, bw_coef_ = 1;  // multiprocessor / memoryBandwidth coefficients (:243)
     size_t spare_mb_ = 200;
     int store_ = CTB_FP32;
     int pad_ = 1;
@@ -114,11 +149,9 @@ class Reconstructor {
     int vol_dims_[3] = {0, 0, 0};
     ctb_timings tm_{};
 
-    // cached device resources
-    cudaStream_t s_copy_ = nullptr, s_comp_ = nullptr, s_down_ = nullptr;
-    DevBuf d_filtered_, d_ring_, d_views_, d_angles_, d_heights_, d_tw_, d_K_, d_slab_[2], d_conv_[2];
-    HostBuf h_stage_[2];
-    int tables_key_[3] = {-1, -1, -1};   // W, pad, filter of the cached tables
+    // cached per-device resources, one entry per active device
+    std::vector<std::unique_ptr<DeviceWork>> workers_;
+    std::mutex progress_mtx_;
 };
 
 }  // namespace ctb

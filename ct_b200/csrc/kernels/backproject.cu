@@ -94,9 +94,9 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ pro
                 if (row_ok(vi, g.vi_hi)) {
                     const int v0 = int(vi);
                     const float fv = __fsub_rn(vi, float(v0));
-                    const T* r0 = col + (long long)v0 * g.W;
+                    const T* r0 = col + (long long)v0 * g.pitch;
                     const float a = (1.0f - fu) * ld(r0) + fu * ld(r0 + 1);
-                    const float b = (1.0f - fu) * ld(r0 + g.W) + fu * ld(r0 + g.W + 1);
+                    const float b = (1.0f - fu) * ld(r0 + g.pitch) + fu * ld(r0 + g.pitch + 1);
                     acc[j] += w * ((1.0f - fv) * a + fv * b);
                 }
             }
@@ -167,6 +167,7 @@ ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, i
     g.zpv = __fmul_rn_host(zPre, g.vs);
     g.vi_hi = float(double(det.height) - 1 - 0.1);
     g.load_scale = load_scale;
+    g.pitch = det.width;
     g.view_stride = (long long)det.width * det.height;
     return g;
 }

@@ -24,7 +24,10 @@
 #include <cuda_fp16.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
+#include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "../ctb_internal.h"
 #include "geom.cuh"
@@ -96,22 +99,42 @@ struct Box {
 constexpr int kConsumerWarps = kTX * kTY / 32;
 constexpr int kThreads = (kConsumerWarps + 1) * 32;
 
-template <typename T, int ZC, int NBUF>
-__global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
-                                                          const T* __restrict__ proj,
-                                                          const float4* __restrict__ views, int n_views,
-                                                          ProjGeom g, Box bx, float* __restrict__ vol,
-                                                          int accumulate) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t full[NBUF];    // box landed (TMA complete_tx)
-    __shared__ __align__(8) uint64_t empty[NBUF];   // every consumer warp finished reading the box
-    __shared__ int2 org[NBUF];                      // box origin (column, row)
-    __shared__ float4 qv[NBUF];                     // {sin, cos, h} of the view in each buffer
-    __shared__ int ovf[NBUF];                       // footprint larger than the box: use global loads
-    __shared__ int abort_flag_s;
-    volatile int& abort_flag = abort_flag_s;  // set by any thread whose bounded wait gave up
-    T* buf = reinterpret_cast<T*>(smem_raw);
+// Pipeline state in shared memory. Barrier phases are tracked through a
+// running box sequence number, so one CTA can run many tiles (persistent
+// kernel) through the same barriers.
+template <int NBUF>
+struct Pipe {
+    uint64_t full[NBUF];    // box landed (TMA complete_tx)
+    uint64_t empty[NBUF];   // every consumer warp finished reading the box
+    int2 org[NBUF];         // box origin (column, row)
+    float4 qv[NBUF];        // {sin, cos, h} of the view in each buffer
+    int ovf[NBUF];          // footprint larger than the box: read global memory
+    int abort_flag;         // a bounded wait gave up
+    long long item;         // persistent kernel: current work item
+};
 
+template <int NBUF>
+__device__ __forceinline__ void pipe_init(Pipe<NBUF>& p) {
+    for (int i = 0; i < NBUF; ++i) {
+        mbar_init(&p.full[i], 1);
+        mbar_init(&p.empty[i], kConsumerWarps);
+    }
+    p.abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool aborted(const volatile int* f) { return *f != 0; }
+
+// One tile (32 x 8 columns x ZC voxels of one slab) over every view.
+// seq: box sequence number of this CTA (identical in all threads), advanced by
+// n_views when the tile loads boxes. Returns false if a bounded wait gave up.
+template <typename T, int ZC, int NBUF>
+__device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __restrict__ proj,
+                                          const float4* __restrict__ views, int n_views, const ProjGeom& g,
+                                          const Box& bx, int buf_stride, float* __restrict__ vol, int accumulate,
+                                          int tile_x, int tile_y, int tile_z, Pipe<NBUF>& p, T* buf,
+                                          unsigned& seq) {
+    volatile int* abort_flag = &p.abort_flag;
     // Consumer warp w covers an 8 (x) x 4 (y) patch of columns: its lanes then
     // sample a compact patch of the box (a few rows x ~12 words), which keeps
     // the shared-memory loads nearly free of bank conflicts even for voxels
@@ -119,7 +142,7 @@ __global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_consta
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const bool producer = warp == kConsumerWarps;
-    const int x0 = blockIdx.x * kTX, y0 = blockIdx.y * kTY, z0 = blockIdx.z * ZC;
+    const int x0 = tile_x * kTX, y0 = tile_y * kTY, z0 = tile_z * ZC;
     const int x = x0 + (warp & 3) * 8 + (lane & 7), y = y0 + ((warp >> 2) & 1) * 4 + (lane >> 3);
     const int x1 = min(x0 + kTX, g.X) - 1, y1 = min(y0 + kTY, g.Y) - 1;
     const int zl = min(ZC, g.Zs - z0);  // voxels of this tile in the slab
@@ -147,32 +170,23 @@ __global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_consta
 #pragma unroll
     for (int j = 0; j < ZC; ++j) zf[j] = float(g.z_begin + z0 + j);
 
-    if (tid == 0) {
-        for (int i = 0; i < NBUF; ++i) {
-            mbar_init(&full[i], 1);
-            mbar_init(&empty[i], kConsumerWarps);
-        }
-        abort_flag = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-
     if (producer) {
         // ------------------------------------------------------------ producer
         int iv = 0;
-        for (; iv < n_views && !abort_flag; ++iv) {
-            const int b = iv % NBUF;
-            // the buffer's previous view (iv - NBUF) must have been read by every consumer warp
-            if (iv >= NBUF) {
+        for (; iv < n_views; ++iv) {
+            const unsigned sq = seq + iv;
+            const int b = sq % NBUF;
+            // the buffer's previous box (sq - NBUF) must have been read by every consumer warp
+            if (sq >= NBUF) {
                 unsigned tries = 0;
-                while (!mbar_try_wait(&empty[b], uint32_t(((iv / NBUF) + 1) & 1))) {
+                while (!mbar_try_wait(&p.empty[b], ((sq / NBUF) + 1) & 1)) {
                     if (++tries > kWaitLimit) {
-                        abort_flag = 1;
+                        *abort_flag = 1;
                         break;
                     }
                 }
-                if (abort_flag) break;
             }
+            if (aborted(abort_flag)) break;
             // footprint of the whole ZC tile (voxels past the slab end are evaluated
             // too and dropped at the store): project the 4 (x, y) corners at both z ends
             float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
@@ -202,26 +216,16 @@ __global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_consta
                 vmin = fminf(fmaxf(vmin, -1.0e6f), 1.0e6f); vmax = fminf(fmaxf(vmax, -1.0e6f), 1.0e6f);
                 const int uo = ((int(floorf(umin)) - 2) >> 3) << 3;   // 16-byte aligned column
                 const int vo = int(floorf(vmin)) - 2;
-                org[b] = make_int2(uo, vo);
-                qv[b] = q;
-                ovf[b] = (int(floorf(umax)) + 3 - uo > bx.BU) || (int(floorf(vmax)) + 3 - vo > bx.BV);
-                mbar_expect_tx(&full[b], uint32_t(bx.BU) * bx.BV * sizeof(T));
+                p.org[b] = make_int2(uo, vo);
+                p.qv[b] = q;
+                p.ovf[b] = (int(floorf(umax)) + 3 - uo > bx.BU) || (int(floorf(vmax)) + 3 - vo > bx.BV);
+                mbar_expect_tx(&p.full[b], uint32_t(bx.BU) * bx.BV * sizeof(T));
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                tma_load_3d(buf + size_t(b) * bx.buf_elems, &map, uo, vo, iv, &full[b]);
+                tma_load_3d(buf + size_t(b) * buf_stride, map, uo, vo, iv, &p.full[b]);
             }
             __syncwarp();
         }
-        __syncthreads();
-        if (abort_flag && lane == 0) {
-            atomicAdd(&g_wait_timeouts, 1u);
-            // bounded drain of every issued box not yet known to have landed before the
-            // CTA's shared memory goes away (the last NBUF issued views)
-            for (int i = max(0, iv - NBUF); i < iv; ++i) {
-                unsigned tries = 0;
-                while (!mbar_try_wait(&full[i % NBUF], uint32_t((i / NBUF) & 1)) && ++tries < kWaitLimit) {
-                }
-            }
-        }
+        seq += iv;  // boxes issued (all of them unless a wait gave up)
         return;
     }
 
@@ -230,18 +234,19 @@ __global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_consta
 #pragma unroll
     for (int j = 0; j < ZC; ++j) acc[j] = 0.0f;
     for (int iv = 0; iv < n_views; ++iv) {
-        const int b = iv % NBUF;
+        const unsigned sq = seq + iv;
+        const int b = sq % NBUF;
         // bounded wait for the box of view iv
         unsigned tries = 0;
-        while (!mbar_try_wait(&full[b], uint32_t((iv / NBUF) & 1))) {
+        while (!mbar_try_wait(&p.full[b], (sq / NBUF) & 1)) {
             if (++tries > kWaitLimit) {
-                abort_flag = 1;
+                *abort_flag = 1;
                 break;
             }
         }
-        if (abort_flag) break;
+        if (aborted(abort_flag)) break;
         if (live) {
-            const float4 q = qv[b];
+            const float4 q = p.qv[b];
             float U, u;
             column_geom(xw, yw, q.x, q.y, g.D, g.uOff, &U, &u);
             if (u >= g.lbU && u <= g.ubU) {
@@ -251,9 +256,9 @@ __global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_consta
                 const float fu = __fsub_rn(ui, float(u0));
                 const RowLine rl = row_line(U, q.z, g.zpv, g.vs, g.vPre);
                 const float vf = row_at(rl, zf[0]), vl = row_at(rl, zf[ZC - 1]);
-                if (!ovf[b]) {
-                    const int2 o = org[b];
-                    const T* col = buf + size_t(b) * bx.buf_elems + (u0 - o.x) - o.y * bx.BU;
+                if (!p.ovf[b]) {
+                    const int2 o = p.org[b];
+                    const T* col = buf + size_t(b) * buf_stride + (u0 - o.x) - o.y * bx.BU;
                     const int BU = bx.BU;
                     // strictly inside the row bounds (half-pixel margin): every voxel of the column passes
                     // the per-voxel test, so this loop and the checked one take the same decisions
@@ -294,9 +299,9 @@ __global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_consta
                         if (row_ok(vi, g.vi_hi)) {
                             const int v0 = int(vi);
                             const float fv = __fsub_rn(vi, float(v0));
-                            const T* r0 = col + (long long)v0 * g.W;
+                            const T* r0 = col + (long long)v0 * g.pitch;
                             const float a = fmaf(fu, gval(r0 + 1) - gval(r0), gval(r0));
-                            const float c = fmaf(fu, gval(r0 + g.W + 1) - gval(r0 + g.W), gval(r0 + g.W));
+                            const float c = fmaf(fu, gval(r0 + g.pitch + 1) - gval(r0 + g.pitch), gval(r0 + g.pitch));
                             acc[j] = fmaf(w, fmaf(fv, c - a, a), acc[j]);
                         }
                     }
@@ -305,18 +310,110 @@ __global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_consta
         }
         // this warp is done with the box of view iv
         __syncwarp();
-        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&empty[b])) : "memory");
+        if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&p.empty[b])) : "memory");
     }
-    __syncthreads();
-    if (abort_flag || x >= g.X || y >= g.Y) return;
+    seq += n_views;
+    if (aborted(abort_flag) || x >= g.X || y >= g.Y) return;
     float* out = vol + (long long)z0 * plane + (long long)y * g.X + x;
 #pragma unroll
     for (int j = 0; j < ZC; ++j) {
         if (j < zl) {
-            float* p = out + j * plane;
-            *p = accumulate ? (*p + acc[j]) : acc[j];
+            float* o = out + j * plane;
+            *o = accumulate ? (*o + acc[j]) : acc[j];
         }
     }
+}
+
+// After an abort: bounded drain of the last NBUF issued boxes (those may still
+// be in flight) before the CTA's shared memory goes away; count the failure.
+template <int NBUF>
+__device__ void pipe_abort_drain(Pipe<NBUF>& p, unsigned seq) {
+    atomicAdd(&g_wait_timeouts, 1u);
+    for (unsigned i = seq > NBUF ? seq - NBUF : 0; i < seq; ++i) {
+        unsigned tries = 0;
+        while (!mbar_try_wait(&p.full[i % NBUF], (i / NBUF) & 1) && ++tries < kWaitLimit) {
+        }
+    }
+}
+
+template <typename T, int ZC, int NBUF>
+__global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+                                                          const T* __restrict__ proj,
+                                                          const float4* __restrict__ views, int n_views,
+                                                          ProjGeom g, Box bx, float* __restrict__ vol,
+                                                          int accumulate) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(16) Pipe<NBUF> p;
+    if (threadIdx.x == 0) pipe_init(p);
+    __syncthreads();
+    unsigned seq = 0;
+    tile_pass<T, ZC, NBUF>(&map, proj, views, n_views, g, bx, bx.buf_elems, vol, accumulate, blockIdx.x,
+                           blockIdx.y, blockIdx.z, p, reinterpret_cast<T*>(smem_raw), seq);
+    __syncthreads();
+    if (threadIdx.x == kConsumerWarps * 32 && p.abort_flag) pipe_abort_drain(p, seq);
+}
+
+// ----------------------------------------------------------------------------
+// Persistent multi-scan kernel: every CTA takes (scan, tile) work items from
+// an atomic counter until the batch is done. Scans may differ in detector
+// size, view count, volume and voxel pitch; each has its own tensor map.
+struct __align__(128) ScanDesc {
+    CUtensorMap map;
+    ProjGeom g;
+    Box bx;
+    const void* proj;
+    const float4* views;
+    float* vol;
+    int n_views;
+    int tiles_x, tiles_y, tiles_z;
+    int accumulate;
+};
+
+template <typename T, int ZC, int NBUF>
+__global__ void __launch_bounds__(kThreads, 4) bp_batch_kernel(const ScanDesc* __restrict__ scans, int n_scans,
+                                                            const long long* __restrict__ tile_start,
+                                                            unsigned long long* queue, int buf_stride) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(16) Pipe<NBUF> p;
+    // the current item's geometry lives in shared memory (read as needed)
+    // rather than in every thread's registers
+    __shared__ ProjGeom sg;
+    __shared__ Box sbx;
+    __shared__ int s_scan, s_tile[3];
+    if (threadIdx.x == 0) pipe_init(p);
+    __syncthreads();
+    const long long total = tile_start[n_scans];
+    unsigned seq = 0;
+    while (true) {
+        if (threadIdx.x == 0) {
+            const long long item = (long long)atomicAdd(queue, 1ull);
+            p.item = item;
+            if (item < total) {
+                int lo = 0, hi = n_scans - 1;  // scan of this item: last s with tile_start[s] <= item
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (tile_start[mid] <= item) lo = mid;
+                    else hi = mid - 1;
+                }
+                const ScanDesc& d = scans[lo];
+                const long long local = item - tile_start[lo];
+                s_scan = lo;
+                s_tile[0] = int(local % d.tiles_x);
+                s_tile[1] = int((local / d.tiles_x) % d.tiles_y);
+                s_tile[2] = int(local / ((long long)d.tiles_x * d.tiles_y));
+                sg = d.g;
+                sbx = d.bx;
+            }
+        }
+        __syncthreads();
+        if (p.item >= total || p.abort_flag) break;
+        const ScanDesc& d = scans[s_scan];
+        tile_pass<T, ZC, NBUF>(&d.map, static_cast<const T*>(d.proj), d.views, d.n_views, sg, sbx, buf_stride,
+                               d.vol, d.accumulate, s_tile[0], s_tile[1], s_tile[2], p,
+                               reinterpret_cast<T*>(smem_raw), seq);
+        __syncthreads();
+    }
+    if (threadIdx.x == kConsumerWarps * 32 && p.abort_flag) pipe_abort_drain(p, seq);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -369,27 +466,41 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     return true;
 }
 
+template <typename T> struct TmaType;
+template <> struct TmaType<float> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; };
+template <> struct TmaType<__half> { static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_FLOAT16; };
+template <> struct TmaType<__nv_bfloat16> {
+    static constexpr CUtensorMapDataType v = CU_TENSOR_MAP_DATA_TYPE_BFLOAT16;
+};
+
+// Tensor map over [n_views][H][W] projections with row pitch g.pitch; columns
+// W..pitch-1 and everything outside the detector read as zero.
 template <typename T>
-int launch_t(const T* proj, CUtensorMapDataType dt, const float4* views, int n_views, const ProjGeom& g,
-             double hmax, float* vol, int accumulate, cudaStream_t s) {
-    constexpr int ZC = 16;
-    Box bx;
-    if (!box_dims(g, ZC, hmax, sizeof(T), &bx)) return CTB_ERR_UNSUPPORTED;
-    if ((g.W * sizeof(T)) % 16 != 0 || (reinterpret_cast<uintptr_t>(proj) & 15) != 0) return CTB_ERR_UNSUPPORTED;
+bool make_map(const T* proj, int n_views, const ProjGeom& g, const Box& bx, CUtensorMap* map) {
+    if ((size_t(g.pitch) * sizeof(T)) % 16 != 0 || (reinterpret_cast<uintptr_t>(proj) & 15) != 0) return false;
     auto enc = encode_fn();
-    if (!enc) return CTB_ERR_UNSUPPORTED;
-    CUtensorMap map;
+    if (!enc) return false;
     const cuuint64_t dims[3] = {cuuint64_t(g.W), cuuint64_t(g.H), cuuint64_t(n_views)};
-    const cuuint64_t strides[2] = {cuuint64_t(g.W) * sizeof(T), cuuint64_t(g.view_stride) * sizeof(T)};
+    const cuuint64_t strides[2] = {cuuint64_t(g.pitch) * sizeof(T), cuuint64_t(g.view_stride) * sizeof(T)};
     const cuuint32_t box[3] = {cuuint32_t(bx.BU), cuuint32_t(bx.BV), 1};
     const cuuint32_t estr[3] = {1, 1, 1};
-    if (enc(&map, dt, 3, const_cast<T*>(proj), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-        return CTB_ERR_UNSUPPORTED;
-    // three box buffers when three CTAs still fit an SM's shared memory, else two
+    return enc(map, TmaType<T>::v, 3, const_cast<T*>(proj), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+               CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// three box buffers when three CTAs still fit an SM's shared memory, else two
+int choose_nbuf(size_t per_buf) { return (3 * (3 * per_buf + 1024) <= 227 * 1024) ? 3 : 2; }
+
+template <typename T, int ZC>
+int launch_t(const T* proj, const float4* views, int n_views, const ProjGeom& g, double hmax, float* vol,
+             int accumulate, cudaStream_t s) {
+    Box bx;
+    if (!box_dims(g, ZC, hmax, sizeof(T), &bx)) return CTB_ERR_UNSUPPORTED;
+    CUtensorMap map;
+    if (!make_map(proj, n_views, g, bx, &map)) return CTB_ERR_UNSUPPORTED;
     const size_t per_buf = size_t(bx.buf_elems) * sizeof(T);
-    const int nbuf = (3 * (3 * per_buf + 1024) <= 227 * 1024) ? 3 : 2;
+    const int nbuf = choose_nbuf(per_buf);
     const size_t smem = size_t(nbuf) * per_buf;
     if (smem > 200 * 1024) return CTB_ERR_UNSUPPORTED;
     auto kern = nbuf == 3 ? bp_tma_kernel<T, ZC, 3> : bp_tma_kernel<T, ZC, 2>;
@@ -400,23 +511,131 @@ int launch_t(const T* proj, CUtensorMapDataType dt, const float4* views, int n_v
     return cuda_status(cudaGetLastError(), "bp_tma_kernel launch");
 }
 
+template <typename T>
+int launch_zc(const void* proj, const float4* views, int n_views, const ProjGeom& g, double hmax, float* vol,
+              int accumulate, int zc, cudaStream_t s) {
+    if (zc == 8) return launch_t<T, 8>((const T*)proj, views, n_views, g, hmax, vol, accumulate, s);
+    return launch_t<T, 16>((const T*)proj, views, n_views, g, hmax, vol, accumulate, s);
+}
+
+// ---------------------------------------------------------------- batch
+template <typename T, int ZC>
+int batch_plan_t(const BpBatchScan* scans, int n, BpBatchPlan* plan) {
+    plan->desc.clear();
+    plan->tile_start.assign(1, 0);
+    plan->included.clear();
+    plan->excluded.clear();
+    int max_elems = 0;
+    // longest items (most views) first, so the last items to finish are short
+    std::vector<int> order(n);
+    for (int i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return scans[a].n_views > scans[b].n_views; });
+    for (int i : order) {
+        const BpBatchScan& sc = scans[i];
+        ScanDesc d;
+        std::memset(&d, 0, sizeof d);
+        // The persistent kernel sizes its buffers for the largest box of the batch;
+        // a scan whose box would push it below four CTAs per SM (three buffers each)
+        // runs through its own launch instead.
+        constexpr size_t kBoxBudget = (227 * 1024 / 4 - 2048) / 3;
+        if (!box_dims(sc.g, ZC, sc.hmax, sizeof(T), &d.bx) || size_t(d.bx.buf_elems) * sizeof(T) > kBoxBudget ||
+            !make_map((const T*)sc.proj, sc.n_views, sc.g, d.bx, &d.map)) {
+            plan->excluded.push_back(i);
+            continue;
+        }
+        d.g = sc.g;
+        d.proj = sc.proj;
+        d.views = sc.views;
+        d.vol = sc.vol;
+        d.n_views = sc.n_views;
+        d.tiles_x = (sc.g.X + kTX - 1) / kTX;
+        d.tiles_y = (sc.g.Y + kTY - 1) / kTY;
+        d.tiles_z = (sc.g.Zs + ZC - 1) / ZC;
+        d.accumulate = sc.accumulate;
+        max_elems = std::max(max_elems, d.bx.buf_elems);
+        const size_t at = plan->desc.size();
+        plan->desc.resize(at + sizeof(ScanDesc));
+        std::memcpy(plan->desc.data() + at, &d, sizeof d);
+        plan->tile_start.push_back(plan->tile_start.back() + (long long)d.tiles_x * d.tiles_y * d.tiles_z);
+        plan->included.push_back(i);
+    }
+    plan->desc_size = sizeof(ScanDesc);
+    plan->total_tiles = plan->tile_start.back();
+    if (plan->included.empty()) return CTB_OK;
+    plan->buf_stride = max_elems;
+    const size_t per_buf = size_t(max_elems) * sizeof(T);
+    plan->nbuf = choose_nbuf(per_buf);
+    plan->smem = size_t(plan->nbuf) * per_buf;
+    if (plan->smem > 200 * 1024) return CTB_ERR_UNSUPPORTED;
+    auto kern = plan->nbuf == 3 ? bp_batch_kernel<T, ZC, 3> : bp_batch_kernel<T, ZC, 2>;
+    CTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(plan->smem)));
+    int per_sm = 0, dev = 0, sms = 0;
+    CTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, plan->smem));
+    CTB_CUDA_TRY(cudaGetDevice(&dev));
+    CTB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    plan->grid = std::max(1, per_sm) * sms;
+    return CTB_OK;
+}
+
+template <typename T>
+int batch_plan_zc(const BpBatchScan* scans, int n, int zc, BpBatchPlan* plan) {
+    if (zc == 8) return batch_plan_t<T, 8>(scans, n, plan);
+    return batch_plan_t<T, 16>(scans, n, plan);
+}
+
+template <typename T, int ZC>
+void batch_launch_t(const BpBatchPlan& plan, const void* desc, const long long* tile_start, int n,
+                    unsigned long long* queue, cudaStream_t s) {
+    auto kern = plan.nbuf == 3 ? bp_batch_kernel<T, ZC, 3> : bp_batch_kernel<T, ZC, 2>;
+    kern<<<plan.grid, kThreads, plan.smem, s>>>(static_cast<const ScanDesc*>(desc), n, tile_start, queue,
+                                                plan.buf_stride);
+}
+
 }  // namespace
 
 int backproject_tma_launch(const void* proj, int store_type, const float4* views, int n_views, const ProjGeom& g,
-                           double hmax, float* vol, int accumulate, cudaStream_t s) {
+                           double hmax, float* vol, int accumulate, cudaStream_t s, int zc) {
     if (n_views <= 0) return CTB_ERR_UNSUPPORTED;
     switch (store_type) {
-        case CTB_FP32:
-            return launch_t((const float*)proj, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, views, n_views, g, hmax, vol,
-                            accumulate, s);
-        case CTB_FP16:
-            return launch_t((const __half*)proj, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, views, n_views, g, hmax, vol,
-                            accumulate, s);
-        case CTB_BF16:
-            return launch_t((const __nv_bfloat16*)proj, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, views, n_views, g, hmax,
-                            vol, accumulate, s);
+        case CTB_FP32: return launch_zc<float>(proj, views, n_views, g, hmax, vol, accumulate, zc, s);
+        case CTB_FP16: return launch_zc<__half>(proj, views, n_views, g, hmax, vol, accumulate, zc, s);
+        case CTB_BF16: return launch_zc<__nv_bfloat16>(proj, views, n_views, g, hmax, vol, accumulate, zc, s);
     }
     return CTB_ERR_UNSUPPORTED;
+}
+
+int bp_batch_plan(int store_type, int zc, const BpBatchScan* scans, int n, BpBatchPlan* plan) {
+    if (n <= 0) return CTB_ERR_ARG;
+    plan->store_type = store_type;
+    plan->zc = zc == 8 ? 8 : 16;
+    switch (store_type) {
+        case CTB_FP32: return batch_plan_zc<float>(scans, n, plan->zc, plan);
+        case CTB_FP16: return batch_plan_zc<__half>(scans, n, plan->zc, plan);
+        case CTB_BF16: return batch_plan_zc<__nv_bfloat16>(scans, n, plan->zc, plan);
+    }
+    return CTB_ERR_ARG;
+}
+
+int bp_batch_launch(const BpBatchPlan& plan, const void* desc, const long long* tile_start, int n,
+                    unsigned long long* queue, cudaStream_t s) {
+    if (n <= 0) return CTB_OK;
+    const bool z8 = plan.zc == 8;
+    switch (plan.store_type) {
+        case CTB_FP32:
+            z8 ? batch_launch_t<float, 8>(plan, desc, tile_start, n, queue, s)
+               : batch_launch_t<float, 16>(plan, desc, tile_start, n, queue, s);
+            break;
+        case CTB_FP16:
+            z8 ? batch_launch_t<__half, 8>(plan, desc, tile_start, n, queue, s)
+               : batch_launch_t<__half, 16>(plan, desc, tile_start, n, queue, s);
+            break;
+        case CTB_BF16:
+            z8 ? batch_launch_t<__nv_bfloat16, 8>(plan, desc, tile_start, n, queue, s)
+               : batch_launch_t<__nv_bfloat16, 16>(plan, desc, tile_start, n, queue, s);
+            break;
+        default: return CTB_ERR_ARG;
+    }
+    return cuda_status(cudaGetLastError(), "bp_batch_kernel launch");
 }
 
 int device_wait_timeouts(unsigned* count, int reset) {

@@ -146,73 +146,144 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// In-place Stockham autosort FFT of length M (power of two) on s[0..M), by TG =
-// M/8 threads (lt = 0..TG-1). Forward: exp(-2 pi i nk/M); inverse: conjugate
-// twiddles, unnormalised. All threads of the CTA must call it (barriers).
+// ------------------------------------------------------ shared-memory FFT
+// Stockham autosort FFT of length M (power of two) by a group of TG = M/8
+// threads: one radix-2 or radix-4 stage (when log2 M is not a multiple of 3)
+// followed by radix-8 stages; every thread owns 8 elements per stage. The
+// last forward stage multiplies by the kernel spectrum on its way to shared
+// memory and the last inverse stage writes the filtered row pair straight to
+// global memory, so each transform costs one shared-memory round trip per
+// stage and no separate passes.
+constexpr float kSqrtHalf = 0.70710678118654752440f;
+
 template <bool INV>
-__device__ void fft_smem(float2* s, int M, int logM, const float2* __restrict__ tw, int lt, int TG) {
-    int Ns = 1;
-    if (logM & 1) {
-        // radix-2 first stage (Ns = 1: no twiddles), 4 butterflies per thread
-        const int nb = M >> 1;
-        float2 y[4][2];
+__device__ __forceinline__ void dft2(float2* v) {
+    const float2 a = v[0], b = v[1];
+    v[0] = make_float2(a.x + b.x, a.y + b.y);
+    v[1] = make_float2(a.x - b.x, a.y - b.y);
+}
+
+// forward: multiply by -i; inverse: by +i
+template <bool INV>
+__device__ __forceinline__ float2 rot90(float2 d) {
+    return INV ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft4(float2& v0, float2& v1, float2& v2, float2& v3) {
+    const float2 a0 = make_float2(v0.x + v2.x, v0.y + v2.y);
+    const float2 a1 = make_float2(v0.x - v2.x, v0.y - v2.y);
+    const float2 a2 = make_float2(v1.x + v3.x, v1.y + v3.y);
+    const float2 a3 = rot90<INV>(make_float2(v1.x - v3.x, v1.y - v3.y));
+    v0 = make_float2(a0.x + a2.x, a0.y + a2.y);
+    v1 = make_float2(a1.x + a3.x, a1.y + a3.y);
+    v2 = make_float2(a0.x - a2.x, a0.y - a2.y);
+    v3 = make_float2(a1.x - a3.x, a1.y - a3.y);
+}
+
+// 8-point DFT in registers: two 4-point DFTs of the even and odd samples joined
+// by the eighth roots of unity.
+template <bool INV>
+__device__ __forceinline__ void dft8(float2* v) {
+    float2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    float2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4<INV>(e0, e1, e2, e3);
+    dft4<INV>(o0, o1, o2, o3);
+    // w^1 = (1 -+ i)/sqrt2, w^2 = -+i, w^3 = (-1 -+ i)/sqrt2 (upper sign: forward)
+    const float2 t1 = INV ? make_float2(kSqrtHalf * (o1.x - o1.y), kSqrtHalf * (o1.x + o1.y))
+                          : make_float2(kSqrtHalf * (o1.x + o1.y), kSqrtHalf * (o1.y - o1.x));
+    const float2 t2 = rot90<INV>(o2);
+    const float2 t3 = INV ? make_float2(-kSqrtHalf * (o3.x + o3.y), kSqrtHalf * (o3.x - o3.y))
+                          : make_float2(kSqrtHalf * (o3.y - o3.x), -kSqrtHalf * (o3.x + o3.y));
+    v[0] = make_float2(e0.x + o0.x, e0.y + o0.y);
+    v[4] = make_float2(e0.x - o0.x, e0.y - o0.y);
+    v[1] = make_float2(e1.x + t1.x, e1.y + t1.y);
+    v[5] = make_float2(e1.x - t1.x, e1.y - t1.y);
+    v[2] = make_float2(e2.x + t2.x, e2.y + t2.y);
+    v[6] = make_float2(e2.x - t2.x, e2.y - t2.y);
+    v[3] = make_float2(e3.x + t3.x, e3.y + t3.y);
+    v[7] = make_float2(e3.x - t3.x, e3.y - t3.y);
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void butterfly(float2* v) {
+    if (R == 2) dft2<INV>(v);
+    else if (R == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+    else dft8<INV>(v);
+}
+
+enum { kFromSmem = 0, kFromInput = 1 };
+enum { kToSmem = 0, kToSmemTimesK = 1, kToOutput = 2 };
+
+// One radix-R stage; each of the TG threads does 8/R butterflies.
+template <int R, bool INV, int SRC, int DST, typename In, typename Out>
+__device__ __forceinline__ void fft_stage(float2* s, int M, int Ns, const float2* __restrict__ tw,
+                                          const float* __restrict__ K, int lt, int TG, const In& in, const Out& out) {
+    constexpr int PER = 8 / R;
+    const int nb = M / R;
+    const int step = M / (Ns * R);
+    float2 y[PER][R];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int b = lt + i * TG;
-            const float2 v0 = s[b], v1 = s[b + nb];
-            y[i][0] = make_float2(v0.x + v1.x, v0.y + v1.y);
-            y[i][1] = make_float2(v0.x - v1.x, v0.y - v1.y);
-        }
-        __syncthreads();
+    for (int i = 0; i < PER; ++i) {
+        const int b = lt + i * TG;
+        const int jm = b & (Ns - 1);
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int b = lt + i * TG;
-            s[2 * b] = y[i][0];
-            s[2 * b + 1] = y[i][1];
-        }
-        __syncthreads();
-        Ns = 2;
-    }
-    const int nb = M >> 2;
-    for (; Ns < M; Ns <<= 2) {
-        float2 y[2][4];
-        const int step = M / (Ns * 4);
+        for (int r = 0; r < R; ++r) y[i][r] = SRC == kFromInput ? in(b + r * nb) : s[b + r * nb];
+        if (Ns > 1) {
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int b = lt + i * TG;
-            const int jm = b & (Ns - 1);
-            float2 v[4];
-#pragma unroll
-            for (int r = 0; r < 4; ++r) v[r] = s[b + r * nb];
-            if (Ns > 1) {
-#pragma unroll
-                for (int r = 1; r < 4; ++r) {
-                    float2 w = __ldg(&tw[(jm * r * step) & (M - 1)]);
-                    if (INV) w.y = -w.y;
-                    v[r] = cmul(v[r], w);
-                }
+            for (int r = 1; r < R; ++r) {
+                float2 w = __ldg(&tw[(jm * r * step) & (M - 1)]);
+                if (INV) w.y = -w.y;
+                y[i][r] = cmul(y[i][r], w);
             }
-            const float2 a0 = make_float2(v[0].x + v[2].x, v[0].y + v[2].y);
-            const float2 a1 = make_float2(v[0].x - v[2].x, v[0].y - v[2].y);
-            const float2 a2 = make_float2(v[1].x + v[3].x, v[1].y + v[3].y);
-            const float2 d = make_float2(v[1].x - v[3].x, v[1].y - v[3].y);
-            // forward: a3 = -i * d ; inverse: a3 = +i * d
-            const float2 a3 = INV ? make_float2(-d.y, d.x) : make_float2(d.y, -d.x);
-            y[i][0] = make_float2(a0.x + a2.x, a0.y + a2.y);
-            y[i][1] = make_float2(a1.x + a3.x, a1.y + a3.y);
-            y[i][2] = make_float2(a0.x - a2.x, a0.y - a2.y);
-            y[i][3] = make_float2(a1.x - a3.x, a1.y - a3.y);
         }
-        __syncthreads();
+        butterfly<R, INV>(y[i]);
+    }
+    if (SRC == kFromSmem && DST != kToOutput) __syncthreads();  // in place: all reads before any write
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const int b = lt + i * TG;
-            const int jm = b & (Ns - 1);
-            const int d0 = (b - jm) * 4 + jm;
+    for (int i = 0; i < PER; ++i) {
+        const int b = lt + i * TG;
+        const int jm = b & (Ns - 1);
+        const int d0 = (b - jm) * R + jm;
 #pragma unroll
-            for (int r = 0; r < 4; ++r) s[d0 + r * Ns] = y[i][r];
+        for (int r = 0; r < R; ++r) {
+            const int idx = d0 + r * Ns;
+            if (DST == kToOutput) {
+                out(idx, y[i][r]);
+            } else if (DST == kToSmemTimesK) {
+                const float k = __ldg(&K[idx]);
+                s[idx] = make_float2(y[i][r].x * k, y[i][r].y * k);
+            } else {
+                s[idx] = y[i][r];
+            }
         }
-        __syncthreads();
+    }
+    if (DST != kToOutput) __syncthreads();
+}
+
+// Whole transform: first stage from SRC0, last stage to DSTL. All threads of
+// the CTA must call it (barriers).
+template <bool INV, int SRC0, int DSTL, typename In, typename Out>
+__device__ void fft_run(float2* s, int M, int logM, const float2* __restrict__ tw, const float* __restrict__ K,
+                        int lt, int TG, const In& in, const Out& out) {
+    const int rem = logM % 3;
+    const int first = rem == 1 ? 2 : rem == 2 ? 4 : 8;
+    const int nst = logM / 3 + (rem ? 1 : 0);
+    int Ns = 1;
+    for (int st = 0; st < nst; ++st) {
+        if (st == 0) {
+            if (nst == 1) fft_stage<8, INV, SRC0, DSTL>(s, M, Ns, tw, K, lt, TG, in, out);
+            else if (first == 2) fft_stage<2, INV, SRC0, kToSmem>(s, M, Ns, tw, K, lt, TG, in, out);
+            else if (first == 4) fft_stage<4, INV, SRC0, kToSmem>(s, M, Ns, tw, K, lt, TG, in, out);
+            else fft_stage<8, INV, SRC0, kToSmem>(s, M, Ns, tw, K, lt, TG, in, out);
+            Ns *= first;
+        } else if (st == nst - 1) {
+            fft_stage<8, INV, kFromSmem, DSTL>(s, M, Ns, tw, K, lt, TG, in, out);
+            Ns *= 8;
+        } else {
+            fft_stage<8, INV, kFromSmem, kToSmem>(s, M, Ns, tw, K, lt, TG, in, out);
+            Ns *= 8;
+        }
     }
 }
 
@@ -234,32 +305,30 @@ __global__ void __launch_bounds__(1024) filter_kernel(const InT* __restrict__ ra
     const long long view = active ? q / pairs : 0;
     const int r0 = active ? int(q - view * pairs) * 2 : 0;
     const bool has1 = r0 + 1 < H;
-    const size_t base0 = (size_t)view * H * W + (size_t)r0 * W;
+    const size_t base0 = (size_t)view * H * W + (size_t)r0 * W;              // raw rows (dense)
+    const size_t obase = (size_t)view * H * a.out_pitch + (size_t)r0 * a.out_pitch;  // filtered rows
 
-    for (int c = lt; c < M; c += TG) {
+    // rows r0 and r0+1 as the real and imaginary parts, zero beyond W
+    auto load = [&](int c) {
         float2 z = make_float2(0.f, 0.f);
         if (active && c < W) {
             z.x = preprocess(raw_value(raw + base0 + c, a), r0, c, a);
             if (has1) z.y = preprocess(raw_value(raw + base0 + W + c, a), r0 + 1, c, a);
         }
-        s[c] = z;
-    }
-    __syncthreads();
-    fft_smem<false>(s, M, a.logM, tw, lt, TG);
-    for (int k = lt; k < M; k += TG) {
-        const float kk = __ldg(&K[k]);
-        float2 z = s[k];
-        s[k] = make_float2(z.x * kk, z.y * kk);
-    }
-    __syncthreads();
-    fft_smem<true>(s, M, a.logM, tw, lt, TG);
-    if (active) {
-        for (int c = lt; c < W; c += TG) {
-            const float2 z = s[c];
-            out[base0 + c] = to_store<OutT>(z.x * a.store_scale);
-            if (has1) out[base0 + W + c] = to_store<OutT>(z.y * a.store_scale);
+        return z;
+    };
+    auto store = [&](int c, float2 z) {
+        if (active && c < W) {
+            out[obase + c] = to_store<OutT>(z.x * a.store_scale);
+            if (has1) out[obase + a.out_pitch + c] = to_store<OutT>(z.y * a.store_scale);
         }
-    }
+    };
+    // preprocessing is kept out of the first FFT stage: done per element here
+    // it keeps the register footprint small (it involves log, sqrt and divide)
+    for (int c = lt; c < M; c += TG) s[c] = load(c);
+    __syncthreads();
+    fft_run<false, kFromSmem, kToSmemTimesK>(s, M, a.logM, tw, K, lt, TG, load, store);
+    fft_run<true, kFromSmem, kToOutput>(s, M, a.logM, tw, K, lt, TG, load, store);
 }
 
 template <typename InT, typename OutT>
@@ -341,6 +410,7 @@ FilterArgs filter_args(const ctb_detector& det, int raw_type, int M, int logM, l
     a.uPre = float(double(det.width) / 2.0);
     a.vPre = float(double(det.height) / 2.0);
     a.store_scale = store_scale;
+    a.out_pitch = det.width;
     return a;
 }
 

@@ -78,7 +78,20 @@ class CtVolume:
         self._ck(lib().ctb_set_skip_projections(self._ctx, value))
 
     def setActiveCudaDevices(self, devices):
-        self._ck(lib().ctb_set_device(self._ctx, int(list(devices)[0])))
+        """Devices that share the reconstruction, each taking a run of z slices;
+        IDs beyond the device count are dropped (a device may be listed twice)."""
+        ids = np.ascontiguousarray(list(devices), np.int32)
+        self._ck(lib().ctb_set_devices(self._ctx, ids.ctypes.data, len(ids)))
+
+    def setGpuCoefficients(self, multiprocessorCoefficient: float, memoryBandwidthCoefficient: float):
+        self._ck(lib().ctb_set_gpu_coefficients(self._ctx, float(multiprocessorCoefficient),
+                                                float(memoryBandwidthCoefficient)))
+
+    def getGpuWeights(self, devices) -> dict:
+        ids = np.ascontiguousarray(list(devices), np.int32)
+        w = np.zeros(len(ids), np.float64)
+        self._ck(lib().ctb_get_gpu_weights(self._ctx, ids.ctypes.data, len(ids), w.ctypes.data))
+        return {int(d): float(x) for d, x in zip(ids, w)}
 
     def setGpuSpareMemory(self, megabytes: int):
         self._ck(lib().ctb_set_gpu_spare_memory(self._ctx, int(megabytes)))
@@ -147,6 +160,14 @@ class CtVolume:
     def saveVolumeToBinaryFile(self, filename: str, indexOrder: int = L.Z_FASTEST, byteOrder: int = L.LITTLE_ENDIAN):
         self._ck(lib().ctb_save_volume(self._ctx, str(filename).encode(), indexOrder, byteOrder))
 
+    def getVolumeCrossSection(self, axis: int, index: int) -> np.ndarray:
+        """Cross section of the last volume, left-handed orientation (Volume::getVolumeCrossSection)."""
+        rows, cols = ctypes.c_int(), ctypes.c_int()
+        self._ck(lib().ctb_get_cross_section(self._ctx, axis, index, None, ctypes.byref(rows), ctypes.byref(cols)))
+        out = np.empty((rows.value, cols.value), np.float32)
+        self._ck(lib().ctb_get_cross_section(self._ctx, axis, index, out.ctypes.data, None, None))
+        return out
+
     def stop(self):
         lib().ctb_stop(self._ctx)
 
@@ -154,3 +175,39 @@ class CtVolume:
         t = L.Timings()
         self._ck(lib().ctb_get_timings(self._ctx, ctypes.byref(t)))
         return t
+
+
+def gpu_weights_from(sm_counts, bandwidths, multiprocessorCoefficient=1.0, memoryBandwidthCoefficient=1.0):
+    """getGpuWeights' formula on given device properties (no device query)."""
+    sm = np.ascontiguousarray(sm_counts, np.int32)
+    bw = np.ascontiguousarray(bandwidths, np.float64)
+    w = np.zeros(len(sm), np.float64)
+    check(lib().ctb_gpu_weights_from(sm.ctypes.data, bw.ctypes.data, len(sm), float(multiprocessorCoefficient),
+                                     float(memoryBandwidthCoefficient), w.ctypes.data))
+    return w
+
+
+def split_slices(weights, z: int) -> np.ndarray:
+    """First slice of each device's z range plus the end (n + 1 entries)."""
+    w = np.ascontiguousarray(weights, np.float64)
+    b = np.zeros(len(w) + 1, np.int32)
+    check(lib().ctb_split_slices(w.ctypes.data, len(w), int(z), b.ctypes.data))
+    return b
+
+
+def read_volume_info(txt_path: str) -> dict:
+    """Dimensions and orders from a reconstruction's .txt info file (as the viewer reads it)."""
+    x, y, z, io, bo = (ctypes.c_int() for _ in range(5))
+    check(lib().ctb_read_volume_info(str(txt_path).encode(), ctypes.byref(x), ctypes.byref(y), ctypes.byref(z),
+                                     ctypes.byref(io), ctypes.byref(bo)))
+    return {"x": x.value, "y": y.value, "z": z.value, "index_order": io.value, "byte_order": bo.value}
+
+
+def load_volume(raw_path: str, x: int, y: int, z: int, index_order: int = L.Z_FASTEST,
+                byte_order: int = L.LITTLE_ENDIAN, data_type: int = 0, header_offset: int = 0,
+                mirror=(False, False, False)) -> np.ndarray:
+    """Volume::loadFromBinaryFile into a (Z, Y, X) float32 array."""
+    out = np.empty((z, y, x), np.float32)
+    check(lib().ctb_load_volume(str(raw_path).encode(), x, y, z, index_order, byte_order, data_type, header_offset,
+                                int(mirror[0]), int(mirror[1]), int(mirror[2]), out.ctypes.data))
+    return out

@@ -121,3 +121,47 @@ def phantom_project(ellipsoids, angles_deg, heights_mm, width, height, pixel_mm,
                                     None if h is None else h.ctypes.data, len(a), width, height, pixel_mm, fcd_mm,
                                     u_offset_mm, ctypes.c_void_p(out.data_ptr()), _stream(stream)))
     return out
+
+
+class Batch:
+    """Many scans of different sizes reconstructed by one persistent
+    backprojection launch under a captured CUDA graph (ctb_batch_*).
+
+    scans: list of dicts with raw (CUDA uint8/uint16/float32 tensor V x H x W),
+    angles_deg, heights_px (or None), det, grid, filter, pad, vol (CUDA float32
+    tensor Z x Y x X, overwritten)."""
+
+    def __init__(self, scans, store=L.FP32, stream=None):
+        self._keep = []
+        arr = (L.Scan * len(scans))()
+        for i, sc in enumerate(scans):
+            a = np.ascontiguousarray(sc["angles_deg"], np.float64)
+            h = None if sc.get("heights_px") is None else np.ascontiguousarray(sc["heights_px"], np.float64)
+            self._keep += [a, h, sc["raw"], sc["vol"]]
+            arr[i] = L.Scan(ctypes.c_void_p(sc["raw"].data_ptr()), RAW_CODES_FN()[sc["raw"].dtype], len(a),
+                            a.ctypes.data, None if h is None else h.ctypes.data, sc["det"], sc["grid"],
+                            sc.get("filter", L.RAMLAK), sc.get("pad", 1), ctypes.c_void_p(sc["vol"].data_ptr()))
+        self._h = ctypes.c_void_p()
+        check(lib().ctb_batch_create(ctypes.byref(self._h), len(scans), arr, store, _stream(stream)))
+
+    def run(self, stream=None):
+        check(lib().ctb_batch_run(self._h, _stream(stream)))
+
+    def run_sequential(self, stream=None):
+        check(lib().ctb_batch_run_sequential(self._h, _stream(stream)))
+
+    def tuning(self):
+        zc, a, b, n = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        check(lib().ctb_batch_tuning(self._h, ctypes.byref(zc), ctypes.byref(a), ctypes.byref(b), ctypes.byref(n)))
+        return {"zc": zc.value, "ms_zc16": a.value, "ms_zc8": b.value, "persistent_scans": n.value}
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value and L._lib is not None:
+            L._lib.ctb_batch_destroy(h)
+            self._h = None
+
+
+def RAW_CODES_FN():
+    _torch()
+    return RAW_CODES

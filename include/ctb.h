@@ -159,6 +159,42 @@ int ctb_forward_project(const float* vol, const double* angles_deg, const double
 int ctb_convert_layout(const float* src, int x, int y, int zs, int index_order, int byte_order,
                        void* dst, void* stream);
 
+/* ------------------------------------------------------ batches of scans */
+
+/* One scan of a batch. Device pointers are the caller's; host arrays are read
+ * during ctb_batch_create only. */
+typedef struct {
+    const void* raw;                  /* device, n_views x H x W raw projections */
+    int32_t raw_type;                 /* CTB_U8 / CTB_U16 / CTB_F32 */
+    int32_t n_views;
+    const double* angles_deg;         /* host, n_views (direction-corrected) */
+    const double* height_offsets_px;  /* host, n_views (relative, pixels) or NULL */
+    ctb_detector det;                 /* radius set (ctb_reference_grid) */
+    ctb_grid grid;
+    int32_t filter;                   /* CTB_RAMLAK / CTB_SHEPPLOGAN / CTB_HANN */
+    int32_t pad;                      /* 1 or 2 */
+    float* vol;                       /* device, X-fastest box volume (overwritten) */
+} ctb_scan;
+
+typedef struct ctb_batch ctb_batch;
+
+/* Many independent scans of different detector, view and volume sizes
+ * reconstructed together: per-scan filtering followed by ONE persistent
+ * backprojection launch whose CTAs take (scan, tile) items from a device work
+ * counter, the whole sequence captured once as a CUDA graph. Allocates the
+ * filtered projections and view tables of every scan, picks the kernel's
+ * z-voxels-per-thread with the built-in autotuner (timing both candidates on
+ * this batch) and captures the graph. No counterpart in the reference, which
+ * reconstructs one scan per process. */
+int ctb_batch_create(ctb_batch** batch, int n_scans, const ctb_scan* scans, int store_type, void* stream);
+int ctb_batch_run(ctb_batch* batch, void* stream);             /* replay the graph */
+int ctb_batch_run_sequential(ctb_batch* batch, void* stream);  /* scan by scan, separate launches */
+/* Autotuner outcome: chosen z voxels per thread, the timed candidates (ms, z = 16 and 8) and how
+ * many scans the persistent kernel takes (scans with voxels so coarse that a tile's footprint box
+ * exceeds the persistent kernel's shared-memory budget get their own launch inside the same graph). */
+int ctb_batch_tuning(const ctb_batch* batch, int* zc, double* ms_zc16, double* ms_zc8, int* n_persistent);
+void ctb_batch_destroy(ctb_batch* batch);
+
 /* ------------------------------------------------------ facade layer */
 
 typedef struct ctb_ctx ctb_ctx;
@@ -191,6 +227,26 @@ int ctb_set_volume_bounds(ctb_ctx* ctx, float xmin, float xmax, float ymin, floa
 int ctb_set_filter(ctb_ctx* ctx, int filter);             /* setFrequencyFilterType */
 int ctb_set_skip_projections(ctb_ctx* ctx, unsigned skip);  /* setSkipProjections */
 int ctb_set_device(ctb_ctx* ctx, int device);             /* setActiveCudaDevices({d}) */
+/* setActiveCudaDevices (Ct/CtVolume.h:107, Ct/CtVolume.cpp:506-520): IDs at or
+ * beyond the device count are dropped; with none left the selection is kept
+ * and CTB_ERR_ARG returned. Each listed device reconstructs its own run of z
+ * slices from all views; a device listed twice runs two workers. */
+int ctb_set_devices(ctb_ctx* ctx, const int* device_ids, int n);
+/* setGpuCoefficients (Ct/CtVolume.h:109-110): exponents of the multiprocessor
+ * and memory-bandwidth shares in the per-device weights. */
+int ctb_set_gpu_coefficients(ctb_ctx* ctx, double multiprocessor_coefficient, double bandwidth_coefficient);
+/* getGpuWeights (Ct/CtVolume.cpp:1353-1381) for the given devices with the
+ * context's coefficients; weights[n] sums to 1. */
+int ctb_get_gpu_weights(ctb_ctx* ctx, const int* device_ids, int n, double* weights);
+/* The same weights from given properties (no device query):
+ * (sm_i/sum sm)^mp * (bw_i/sum bw)^bwc, normalised. */
+int ctb_gpu_weights_from(const int* sm_count, const double* bandwidth, int n, double multiprocessor_coefficient,
+                         double bandwidth_coefficient, double* weights);
+/* Slice split of launchCudaThreads (Ct/CtVolume.cpp:1339-1344): device i gets
+ * [begin[i], begin[i+1]) with round(weight_i * z) slices, clamped to z; the
+ * last device also takes what rounding left over (the reference can leave
+ * slices unassigned there). begin has n + 1 entries. */
+int ctb_split_slices(const double* weights, int n, int z, int* begin);
 int ctb_set_gpu_spare_memory(ctb_ctx* ctx, size_t megabytes);  /* setGpuSpareMemory */
 /* Engine extensions (no reference counterpart). */
 int ctb_set_precision(ctb_ctx* ctx, int store_type);      /* CTB_FP32 / FP16 / BF16 */
@@ -238,6 +294,34 @@ typedef struct {
     double voxel_views;     /* x*y*z*views processed */
 } ctb_timings;
 int ctb_get_timings(const ctb_ctx* ctx, ctb_timings* t);
+
+/* ------------------------------------------------------ volume files */
+
+/* DataType, Common/types.h:27-36 (same order). */
+enum { CTB_DT_FLOAT32 = 0, CTB_DT_DOUBLE64, CTB_DT_UINT8, CTB_DT_INT8, CTB_DT_UINT16, CTB_DT_INT16,
+       CTB_DT_UINT32, CTB_DT_INT32 };
+
+/* Axis, Common/Volume.h:18-22. */
+enum { CTB_AXIS_X = 0, CTB_AXIS_Y = 1, CTB_AXIS_Z = 2 };
+
+/* Read the dimensions, byte order and index order from a reconstruction's
+ * .txt info file, as the viewer does (CtViewer/ViewerInterface.cpp:486-523):
+ * lines containing "X size:", "Y size:", "Z size:", "Byte order:" ("Big
+ * endian") and "Index order:" ("X fastest"), case-insensitive. CTB_ERR_ARG if
+ * any of the five is missing. */
+int ctb_read_volume_info(const char* txt_path, int* x, int* y, int* z, int* index_order, int* byte_order);
+
+/* Volume<float>::loadFromBinaryFile (Common/Volume.h:336-472): read x*y*z
+ * samples of data_type after header_offset bytes in index_order / byte_order,
+ * optionally mirrored per axis, into an X-fastest float volume. */
+int ctb_load_volume(const char* raw_path, int x, int y, int z, int index_order, int byte_order, int data_type,
+                    size_t header_offset, int mirror_x, int mirror_y, int mirror_z, float* out_xfastest);
+
+/* Volume::getVolumeCrossSection with the left-handed orientation CtVolume
+ * uses (Common/Volume.h:577-648, Ct/CtVolume.cpp:391-393) of the last
+ * reconstructed volume: axis X -> Z rows x Y columns, Y -> Z x X, Z -> X x Y.
+ * out holds rows*cols floats (row-major); rows/cols are returned. */
+int ctb_get_cross_section(const ctb_ctx* ctx, int axis, int index, float* out, int* rows, int* cols);
 
 /* ------------------------------------------------------ synthetic data */
 

@@ -319,3 +319,25 @@ def test_gradient_finite_differences():
         gi = float(g[k, j, i])
         assert abs(fd - gi) <= 1e-4 * max(1.0, abs(fd)), ((k, j, i), fd, gi)
     del base
+
+
+def test_save_load_round_trip_and_cross_sections(tmp_path):
+    from ct_b200 import load_volume, read_volume_info
+    csv, imgs, geom = c1_scan(tmp_path, n_views=20, W=48, H=36)
+    v = CtVolume(csv)
+    v.setVolumeBounds(0.0, 1.0, 0.1, 0.9, 0.2, 0.8)
+    v.reconstructVolume()
+    zyx = v.volume(L.X_FASTEST)
+    for order, endian in [(L.Z_FASTEST, L.BIG_ENDIAN), (L.X_FASTEST, L.LITTLE_ENDIAN)]:
+        raw = tmp_path / f"rt_{order}_{endian}.raw"
+        v.saveVolumeToBinaryFile(str(raw), order, endian)
+        info = read_volume_info(tmp_path / f"rt_{order}_{endian}.txt")
+        assert (info["x"], info["y"], info["z"]) == v.grid().box
+        assert (info["index_order"], info["byte_order"]) == (order, endian)
+        back = load_volume(raw, info["x"], info["y"], info["z"], info["index_order"], info["byte_order"])
+        assert np.array_equal(back, zyx)
+    Z, Y, X = zyx.shape
+    # left-handed cross sections (Common/Volume.h:577-648)
+    assert np.array_equal(v.getVolumeCrossSection(2, Z // 2), zyx[Z // 2].T)             # rows x, cols y
+    assert np.array_equal(v.getVolumeCrossSection(0, X // 3), zyx[::-1, :, X // 3])       # rows z (flipped), cols y
+    assert np.array_equal(v.getVolumeCrossSection(1, Y // 2), zyx[::-1, Y // 2, ::-1])    # rows z (flipped), cols x (flipped)

@@ -297,10 +297,12 @@ def voxelise_gpu(ellipsoids, edge, voxel_mm):
 
 def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
     """C4: matched forward projector A and backprojector A^T on a 512^3 float32 volume, 360 views of
-    512x512. Dot-product test <Ax, y> = <x, A^T y> with seeded Gaussian x, y; central finite differences of
-    f(x) = ||Ax - p||^2 on 64 random voxels against 2 A^T (Ax - p) (A(x +- eps e_i) = Ax +- eps A e_i, with
-    A e_i projected from a one-slice slab holding the voxel); then 20 steepest-descent iterations with exact
-    line search from the FDK reconstruction of a 20-ellipsoid phantom with Poisson noise at 1e4 photons."""
+    512x512. Dot-product test <Ax, y> = <x, A^T y> with seeded Gaussian x, y; device time of A and A^T;
+    central finite differences of f(x) = ||Ax - p||^2 on 64 random voxels against 2 A^T (Ax - p)
+    (A(x +- eps e_i) = Ax +- eps A e_i, with A e_i projected from a one-slice slab holding the voxel);
+    then 20 steepest-descent iterations with exact line search. The data are consistent with the model:
+    p = A(truth) + 1 % Gaussian noise, truth the voxelised 20-ellipsoid phantom; the start is the FDK
+    reconstruction (hann) of the phantom's analytic projections (Poisson noise at 1e4 photons), scaled to p."""
     import torch
 
     from ct_b200 import ops, synth
@@ -309,7 +311,8 @@ def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
     d, _ = ops.detector(det, det, float(np.float32(geom.fcd_px)))
     grid = ops.custom_grid(d, (edge, edge, edge), 1.0)
     ang = geom.angles()
-    out = {"volume": [edge] * 3, "views": views, "detector": [det, det]}
+    units = float(edge) ** 3 * views
+    out = {"volume": [edge] * 3, "views": views, "detector": [det, det], "voxel_views_per_op": units}
     t0 = time.perf_counter()
     g = torch.Generator(device="cuda").manual_seed(seed)
     x = torch.randn((edge, edge, edge), device="cuda", generator=g)
@@ -318,18 +321,40 @@ def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
     Aty = ops.backproject(y, ang, None, d, grid)
     lhs, rhs = float((Ax.double() * y.double()).sum()), float((x.double() * Aty.double()).sum())
     out["dot_test_rel"] = abs(lhs - rhs) / max(abs(lhs), abs(rhs))
+    # device time of one A and one A^T (CUDA events, after the warm-up above)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    reps = 3
+    ev[0].record()
+    for _ in range(reps):
+        ops.forward_project(x, ang, None, d, grid, out=Ax)
+    ev[1].record()
+    for _ in range(reps):
+        ops.backproject(y, ang, None, d, grid, out=Aty)
+    ev[2].record()
+    torch.cuda.synchronize()
+    fp_ms, bp_ms = ev[0].elapsed_time(ev[1]) / reps, ev[1].elapsed_time(ev[2]) / reps
+    out.update({"forward_ms": fp_ms, "forward_gups": units / fp_ms / 1e6,
+                "backproject_fp32_ms": bp_ms, "backproject_fp32_gups": units / bp_ms / 1e6})
     del Ax, Aty, y
-    # data: noisy analytic phantom, line integrals in detector-pixel units
+    # data consistent with the model: A(truth) + noise
     scan = synth.make_scan(geom, 20, seed=seed, photons=1e4)
-    p = -torch.log(torch.clamp(scan.images.float(), min=1.0) / 65535.0) / (0.02 * geom.pixel_eff)
-    # FDK start (ramlak, FP32), rescaled to the data by least squares
-    filt = ops.filter_projections(scan.images, d, L.RAMLAK, 1, L.FP32)
+    truth = voxelise_gpu(scan.ellipsoids, edge, geom.pixel_eff)
+    p = ops.forward_project(truth, ang, None, d, grid)
+    p.add_(torch.randn(p.shape, device="cuda", generator=g), alpha=0.01 * float(p.double().pow(2).mean().sqrt()))
+    # FDK start (hann, FP32) from the analytic noisy projections, scaled to the data by least squares
+    filt = ops.filter_projections(scan.images, d, L.HANN, 1, L.FP32)
     x = ops.backproject(filt, ang, None, d, grid)
     del filt
     Ax = ops.forward_project(x, ang, None, d, grid)
     c = float((Ax.double() * p.double()).sum() / (Ax.double() * Ax.double()).sum())
     x.mul_(c)
     r = Ax.mul_(c).sub_(p)
+
+    def err_to_truth(v):
+        vs = v.double()
+        s_fit = float((vs * truth).sum() / (vs * vs).sum())
+        return float((s_fit * vs - truth).norm() / truth.norm())
+
     # finite differences on 64 voxels
     grad = 2.0 * ops.backproject(r, ang, None, d, grid)
     rng = np.random.default_rng(seed)
@@ -345,9 +370,11 @@ def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
         fd = (fp - fm) / (2 * eps)
         gi = float(grad[k, j, i])
         worst = max(worst, abs(fd - gi) / max(abs(fd), 1e-12))
+    del grad
     out["fd_max_rel_err_64_voxels"] = worst
     # steepest descent with exact line search on the quadratic
     res0 = float(r.double().norm() / p.double().norm())
+    err0 = err_to_truth(x)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     for _ in range(iters):
@@ -360,12 +387,8 @@ def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
     torch.cuda.synchronize()
     t_it = (time.perf_counter() - t1) / iters
     res = float(r.double().norm() / p.double().norm())
-    # error to the voxelised phantom (after the best scalar fit of the units)
-    truth = voxelise_gpu(scan.ellipsoids, edge, geom.pixel_eff)
-    xs = x.double()
-    s_fit = float((xs * truth).sum() / (xs * xs).sum())
     out.update({"data_residual_rel_start": res0, "data_residual_rel_after": res, "iterations": iters,
-                "rel_l2_to_phantom_after": float((s_fit * xs - truth).norm() / truth.norm()),
+                "rel_l2_to_phantom_start": err0, "rel_l2_to_phantom_after": err_to_truth(x),
                 "seconds_per_iteration": t_it, "seconds_total": time.perf_counter() - t0})
     del x, r, p, truth, scan
     torch.cuda.empty_cache()

@@ -18,6 +18,7 @@ STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_IO", 3: "ERR_CSV", 4: "ERR_IMAGE"
                 7: "ERR_TIMEOUT", 8: "INTERRUPTED", 9: "ERR_UNSUPPORTED"}
 RAMLAK, SHEPPLOGAN, HANN = 0, 1, 2
 X_FASTEST, Z_FASTEST = 0, 1
+AXIS_X, AXIS_Y, AXIS_Z = 0, 1, 2
 LITTLE_ENDIAN, BIG_ENDIAN = 0, 1
 FP32, FP16, BF16 = 0, 1, 2
 U8, U16, F32 = 8, 16, 32
@@ -51,6 +52,8 @@ class Timings(ctypes.Structure):
 
 
 PROGRESS_CB = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_double, ctypes.c_void_p)
+PREVIEW_CB = ctypes.CFUNCTYPE(None, ctypes.c_double, ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int,
+                              ctypes.c_void_p)
 
 # name -> (restype, argtypes)
 P, I, F, D, Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_size_t
@@ -100,6 +103,10 @@ SIGNATURES = {
     "ctb_read_volume_info": (I, [ctypes.c_char_p, P, P, P, P, P]),
     "ctb_load_volume": (I, [ctypes.c_char_p, I, I, I, I, I, I, Z, I, I, I, P]),
     "ctb_get_cross_section": (I, [P, I, I, P, P, P]),
+    "ctb_set_cross_section_axis": (I, [P, I]),
+    "ctb_set_cross_section_index": (I, [P, I]),
+    "ctb_get_cross_section_info": (I, [P, P, P, P]),
+    "ctb_set_preview_callback": (I, [P, PREVIEW_CB, P]),
     "ctb_batch_create": (I, [P, I, P, I, P]),
     "ctb_batch_run": (I, [P, P]),
     "ctb_batch_run_sequential": (I, [P, P]),

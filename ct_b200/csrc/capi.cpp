@@ -301,6 +301,26 @@ int ctb_save_volume(ctb_ctx* ctx, const char* path, int index_order, int byte_or
     return ctx->r.save(path, index_order, byte_order);
 }
 
+int ctb_set_cross_section_axis(ctb_ctx* ctx, int axis) {
+    CTX_CHECK(ctx);
+    return ctx->r.set_cross_section_axis(axis);
+}
+int ctb_set_cross_section_index(ctb_ctx* ctx, int index) {
+    CTX_CHECK(ctx);
+    return ctx->r.set_cross_section_index(index);
+}
+int ctb_get_cross_section_info(const ctb_ctx* ctx, int* axis, int* index, int* size) {
+    CTX_CHECK(ctx);
+    if (axis) *axis = ctx->r.cross_section_axis();
+    if (index) *index = ctx->r.cross_section_index();
+    if (size) *size = ctx->r.cross_section_size();
+    return CTB_OK;
+}
+int ctb_set_preview_callback(ctb_ctx* ctx, ctb_preview_cb cb, void* user) {
+    CTX_CHECK(ctx);
+    ctx->r.set_preview(cb, user);
+    return CTB_OK;
+}
 int ctb_get_cross_section(const ctb_ctx* ctx, int axis, int index, float* out, int* rows, int* cols) {
     CTX_CHECK(ctx);
     if (axis < CTB_AXIS_X || axis > CTB_AXIS_Z) return arg_error("unknown axis");

@@ -207,6 +207,42 @@ void Reconstructor::update_grid() {
     g.y_from = int(unsigned(rel_[2] * g.y_size + 0.5)); g.y_to = int(unsigned(rel_[3] * g.y_size + 0.5));
     g.z_from = int(unsigned(rel_[4] * g.z_size + 0.5)); g.z_to = int(unsigned(rel_[5] * g.z_size + 0.5));
     grid_ = g;
+    // keep the cross-section index inside the box (:1411-1417)
+    const int ext = box_extent(cs_axis_);
+    if (cs_index_ >= ext) cs_index_ = ext / 2;
+}
+
+int Reconstructor::box_extent(int axis) const {
+    if (axis == CTB_AXIS_X) return grid_.x_to - grid_.x_from;
+    if (axis == CTB_AXIS_Y) return grid_.y_to - grid_.y_from;
+    return grid_.z_to - grid_.z_from;
+}
+
+int Reconstructor::cross_section_size() const { return std::max(0, box_extent(cs_axis_)); }
+
+// setCrossSectionAxis (:401-410): the index moves to the middle of the axis.
+int Reconstructor::set_cross_section_axis(int axis) {
+    if (axis < CTB_AXIS_X || axis > CTB_AXIS_Z) return fail(CTB_ERR_ARG, "unknown axis");
+    cs_axis_ = axis;
+    cs_index_ = std::max(0, box_extent(axis)) / 2;
+    return CTB_OK;
+}
+
+// setCrossSectionIndex (:395-399): ignored unless inside the box.
+int Reconstructor::set_cross_section_index(int index) {
+    if (index >= 0 && index < box_extent(cs_axis_)) cs_index_ = index;
+    return CTB_OK;
+}
+
+// reconstructionProgress / reconstructionFinished with the cross section of
+// the volume as it stands (Ct/CtVolume.cpp:952, :1479-1483, :615).
+void Reconstructor::emit_preview(const float* vol, double pct) {
+    const int X = grid_.x_to - grid_.x_from, Y = grid_.y_to - grid_.y_from, Z = grid_.z_to - grid_.z_from;
+    int rows = 0, cols = 0;
+    if (cross_section_of(vol, X, Y, Z, cs_axis_, cs_index_, nullptr, &rows, &cols) != CTB_OK) return;
+    preview_buf_.resize(size_t(rows) * cols);
+    cross_section_of(vol, X, Y, Z, cs_axis_, cs_index_, preview_buf_.data(), nullptr, nullptr);
+    preview_(pct, preview_buf_.data(), rows, cols, preview_user_);
 }
 
 // setVolumeBounds (Ct/CtVolume.cpp:487-500), including the reference's clamp
@@ -467,6 +503,7 @@ int Reconstructor::assign_scan(const void* images, int raw_type, int n_views, in
     }
     have_scan_ = true;
     update_grid();
+    cs_index_ = std::max(0, box_extent(cs_axis_)) / 2;  // (:317-326)
     return CTB_OK;
 }
 
@@ -486,6 +523,12 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
                         "The memory allocation for the volume failed. Maybe there is not enought free RAM.");
         target = static_cast<float*>(volume_.p);
         index_order = CTB_X_FASTEST;
+        if (preview_) {  // previews show the unfinished part as zeros (reinitialise, :555)
+            const size_t n = size_t(X) * Y * Z, parts = 16;
+            parallel_for(parts, [&](size_t p) {
+                std::memset(target + p * n / parts, 0, sizeof(float) * ((p + 1) * n / parts - p * n / parts));
+            });
+        }
     }
 
     // one worker per active device entry; workers keep their buffers while
@@ -529,7 +572,10 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
         if (!host_out) vol_dims_[0] = vol_dims_[1] = vol_dims_[2] = 0;  // volume.clear() (:617)
         return fail(status, msg);
     }
-    if (!host_out) { vol_dims_[0] = X; vol_dims_[1] = Y; vol_dims_[2] = Z; }
+    if (!host_out) {
+        vol_dims_[0] = X; vol_dims_[1] = Y; vol_dims_[2] = Z;
+        if (preview_) emit_preview(target, 100.0);  // reconstructionFinished (:615)
+    }
 
     ctb_timings t{};
     for (auto& w : workers_) {
@@ -547,12 +593,13 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
 
 // emitGlobalCudaProgress (Ct/CtVolume.cpp:1469-1485): the total is each
 // worker's completion weighted by its share of the slices.
-void Reconstructor::worker_progress(DeviceWork& w, double frac) {
+void Reconstructor::worker_progress(DeviceWork& w, double frac, const float* preview_vol) {
     std::lock_guard<std::mutex> lk(progress_mtx_);
     w.progress = frac;
     double total = 0;
     for (auto& o : workers_) total += o->progress * o->share;
     progress(1, 100.0 * total);
+    if (preview_ && preview_vol) emit_preview(preview_vol, 100.0 * total);
 }
 
 // Reconstructs box slices [z_lo, z_hi) on worker w's device into out, which
@@ -795,7 +842,11 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         }
         if (ce != cudaSuccess) return cuda_fail("volume download");
         cudaEventRecord(ev_down[b], w.s_down);
-        worker_progress(w, double(k + 1) / double(nslabs));
+        // previews read the context's own volume up to the previous slab, which
+        // has landed by now (waiting for this one would stall the next launch)
+        const bool preview = preview_ && out == static_cast<float*>(volume_.p) && out_pinned && k >= 1;
+        if (preview) cudaEventSynchronize(ev_down[(k - 1) % 2]);
+        worker_progress(w, double(k + 1) / double(nslabs), preview ? out : nullptr);
     }
     cudaEventRecord(e_b1, w.s_comp);
     if (!out_pinned)

@@ -24,6 +24,10 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+// Cross section of an X-fastest X x Y x Z volume in the left-handed
+// orientation (Common/Volume.h:577-648); out == nullptr only reports the size.
+int cross_section_of(const float* vol, int X, int Y, int Z, int axis, int index, float* out, int* rows, int* cols);
+
 // Page-locked host buffer.
 struct HostBuf {
     void* p = nullptr;
@@ -85,6 +89,12 @@ class Reconstructor {
     int set_grid(int x, int y, int z, float vs);
     int set_slab(int s) { slab_req_ = s; return CTB_OK; }
     void set_progress(ctb_progress_cb cb, void* user) { cb_ = cb; cb_user_ = user; }
+    void set_preview(ctb_preview_cb cb, void* user) { preview_ = cb; preview_user_ = user; }
+    int set_cross_section_axis(int axis);
+    int set_cross_section_index(int index);
+    int cross_section_axis() const { return cs_axis_; }
+    int cross_section_index() const { return cs_index_; }
+    int cross_section_size() const;
 
     // ---- getters
     const ctb_detector& detector() const { return det_; }
@@ -110,7 +120,9 @@ class Reconstructor {
     void update_grid();
     int run_pipeline(DeviceWork& w, float* host_out, int index_order, int z_lo, int z_hi);
     void progress(int stage, double pct) { if (cb_) cb_(stage, pct, cb_user_); }
-    void worker_progress(DeviceWork& w, double frac);
+    void worker_progress(DeviceWork& w, double frac, const float* preview_vol = nullptr);
+    void emit_preview(const float* vol, double pct);
+    int box_extent(int axis) const;
 
     std::mutex mtx_;                 // exclusiveFunctionsMutex (Ct/CtVolume.h:258)
     std::atomic<bool> stop_{false};  // stopActiveProcess (:245)
@@ -140,6 +152,11 @@ class Reconstructor {
     float rel_[6] = {0, 1, 0, 1, 0, 1};
     ctb_progress_cb cb_ = nullptr;
     void* cb_user_ = nullptr;
+    ctb_preview_cb preview_ = nullptr;
+    void* preview_user_ = nullptr;
+    std::vector<float> preview_buf_;
+    int cs_axis_ = CTB_AXIS_Z;       // crossSectionAxis (:239)
+    int cs_index_ = 0;               // crossSectionIndex (:238)
 
     // geometry (updateBoundaries)
     ctb_grid grid_{};

@@ -62,10 +62,7 @@ float convert(const unsigned char* p, int dt, bool swap) {
 
 }  // namespace
 
-int Reconstructor::cross_section(int axis, int index, float* out, int* rows, int* cols) const {
-    const int X = vol_dims_[0], Y = vol_dims_[1], Z = vol_dims_[2];
-    if (X == 0 || !volume_.p) return CTB_ERR_ARG;
-    const float* v = static_cast<const float*>(volume_.p);  // X-fastest
+int cross_section_of(const float* v, int X, int Y, int Z, int axis, int index, float* out, int* rows, int* cols) {
     auto at = [&](size_t x, size_t y, size_t z) { return v[(z * Y + y) * X + x]; };
     int R, C;
     if (axis == CTB_AXIS_X) { R = Z; C = Y; if (index < 0 || index >= X) return CTB_ERR_ARG; }
@@ -83,6 +80,12 @@ int Reconstructor::cross_section(int axis, int index, float* out, int* rows, int
             out[size_t(r) * C + c] = val;
         }
     return CTB_OK;
+}
+
+int Reconstructor::cross_section(int axis, int index, float* out, int* rows, int* cols) const {
+    const int X = vol_dims_[0], Y = vol_dims_[1], Z = vol_dims_[2];
+    if (X == 0 || !volume_.p) return CTB_ERR_ARG;
+    return cross_section_of(static_cast<const float*>(volume_.p), X, Y, Z, axis, index, out, rows, cols);
 }
 
 }  // namespace ctb

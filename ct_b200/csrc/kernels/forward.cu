@@ -9,14 +9,20 @@
 // voxels with u0 in {c-1, c} and v0 in {r-1, r} of
 //     w * (u0 == c ? 1-fu : fu) * (v0 == r ? 1-fv : fv) * vol.
 //
-// Ray-driven gather (deterministic, no atomics): one thread per detector pixel,
-// lanes of a warp along detector rows of one column so that the column search
-// is uniform across the warp. The thread walks the in-plane axis that is most
-// perpendicular to the ray; for each position it solves u(x, y) = c-1-W/2 and
-// c+1-W/2 for the other axis (u is a ratio of linear functions), visits the
-// few candidate columns in between, re-evaluates every quantity with the very
-// same FP32 expressions as the backprojector (so the discrete decisions u0, v0
-// and the masks agree bit for bit) and adds the voxels whose rows fall on r.
+// Ray-driven gather (deterministic, no atomics). A warp owns 32 consecutive
+// detector rows of one detector column c of one view; everything that depends
+// only on (view, c) -- which voxel columns can reach c -- is shared by the
+// warp instead of being recomputed per lane:
+//  1. the warp walks the in-plane axis that is most perpendicular to the ray,
+//     32 positions at a time, one position per lane; each lane solves
+//     u(x, y) = c-1-W/2 and c+1-W/2 for the other axis (u is a ratio of linear
+//     functions) and gets a short range of candidate columns;
+//  2. step by step through those ranges, each lane evaluates one candidate
+//     column with the very same FP32 expressions as the backprojector (so the
+//     discrete decisions u0, v0 and the masks agree bit for bit);
+//  3. the columns that reach c are broadcast one at a time (ballot + shuffles)
+//     and every lane adds the one to three voxels of that column whose rows
+//     fall on its own detector row r.
 // The volume is read in a z-fastest copy so that a warp's lanes (consecutive
 // rows -> consecutive z) read contiguous memory.
 
@@ -28,14 +34,16 @@ namespace ctb {
 namespace {
 
 constexpr int kFR = 32, kFC = 8;
+constexpr unsigned kAll = 0xffffffffu;
 
 __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__ volz,
                                                        const float4* __restrict__ views, ProjGeom g,
                                                        float* __restrict__ proj, int accumulate) {
-    const int r = blockIdx.x * kFR + threadIdx.x;
+    const int lane = threadIdx.x;
+    const int r = blockIdx.x * kFR + lane;
     const int c = blockIdx.y * kFC + threadIdx.y;
     const int iv = blockIdx.z;
-    if (c >= g.W) return;
+    if (c >= g.W) return;  // whole warps leave together
     const float4 q = __ldg(&views[iv]);
     const float sn = q.x, cs = q.y, h = q.z;
     const float D = g.D;
@@ -45,56 +53,89 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
     const int ns = x_major ? g.Y : g.X;
     const float ppre = x_major ? g.xPre : g.yPre;
     const float spre = x_major ? g.yPre : g.xPre;
+    const float rf = float(r);
     float acc = 0.0f;
-    for (int ip = 0; ip < np; ++ip) {
-        const float pw = (float(ip) - ppre) * g.vs;
-        // secondary world coordinate where u takes the values Tlo / Thi
-        double s_a, s_b;
-        if (x_major) {  // y = [T (D - x cs) + D (x sn - uOff)] / (D cs + T sn)
-            s_a = (Tlo * (D - pw * cs) + D * (pw * sn - g.uOff)) / (D * cs + Tlo * sn);
-            s_b = (Thi * (D - pw * cs) + D * (pw * sn - g.uOff)) / (D * cs + Thi * sn);
-        } else {        // x = [T (D - y sn) - D (y cs + uOff)] / (T cs - D sn)
-            s_a = (Tlo * (D - pw * sn) - D * (pw * cs + g.uOff)) / (Tlo * cs - D * sn);
-            s_b = (Thi * (D - pw * sn) - D * (pw * cs + g.uOff)) / (Thi * cs - D * sn);
+    for (int ip0 = 0; ip0 < np; ip0 += 32) {
+        // (1) candidate range of this lane's position
+        const int ip = ip0 + lane;
+        int i0 = 0, cnt = 0;
+        if (ip < np) {
+            const float pw = (float(ip) - ppre) * g.vs;
+            double s_a, s_b;
+            if (x_major) {  // y = [T (D - x cs) + D (x sn - uOff)] / (D cs + T sn)
+                s_a = (Tlo * (D - pw * cs) + D * (pw * sn - g.uOff)) / (D * cs + Tlo * sn);
+                s_b = (Thi * (D - pw * cs) + D * (pw * sn - g.uOff)) / (D * cs + Thi * sn);
+            } else {        // x = [T (D - y sn) - D (y cs + uOff)] / (T cs - D sn)
+                s_a = (Tlo * (D - pw * sn) - D * (pw * cs + g.uOff)) / (Tlo * cs - D * sn);
+                s_b = (Thi * (D - pw * sn) - D * (pw * cs + g.uOff)) / (Thi * cs - D * sn);
+            }
+            const double lo = fmin(s_a, s_b) / g.vs + spre, hi = fmax(s_a, s_b) / g.vs + spre;
+            // (clamped to [-2, ns + 2] first: the int conversions stay in range
+            // for rays nearly parallel to the secondary axis, NaN gives the full range)
+            const double big = double(ns) + 2.0;
+            i0 = int(fmax(0.0, floor(fmin(fmax(lo, -2.0), big)) - 1.0));
+            const int i1 = int(fmin(double(ns - 1), ceil(fmax(fmin(hi, big), -2.0)) + 1.0));
+            cnt = max(0, i1 - i0 + 1);
         }
-        const double lo = fmin(s_a, s_b) / g.vs + spre, hi = fmax(s_a, s_b) / g.vs + spre;
-        const int i0 = max(0, int(floor(lo)) - 1);
-        const int i1 = min(ns - 1, int(ceil(hi)) + 1);
-        for (int is = i0; is <= i1; ++is) {
-            const int x = x_major ? ip : is, y = x_major ? is : ip;
-            const float xw = world_coord(x, g.xPre, g.vs);
-            const float yw = world_coord(y, g.yPre, g.vs);
-            if (!in_cylinder(xw, yw, g.r2)) continue;
-            float U, u;
-            column_geom(xw, yw, sn, cs, D, g.uOff, &U, &u);
-            if (!(u >= g.lbU && u <= g.ubU)) continue;
-            const float ui = __fadd_rn(u, g.uPre);
-            const int u0 = int(ui);
-            const float fu = __fsub_rn(ui, float(u0));
-            float bu;
-            if (u0 == c) bu = 1.0f - fu;
-            else if (u0 + 1 == c) bu = fu;
-            else continue;
-            const float w = __fmul_rn(__fmul_rn(U, U), g.load_scale);
-            // rows: vi(z) = c0 + z mdv in [r-1, r+1)  ->  z range (mdv < 0)
-            const float* col = volz + ((long long)x * g.Y + y) * g.Zs;
-            const RowLine rl = row_line(U, h, g.zpv, g.vs, g.vPre);
-            const double dv = -double(rl.mdv);
-            // (box z index = slab-local z + z_begin)
-            const double zlo = (double(rl.c0) - (r + 1)) / dv - g.z_begin;
-            const double zhi = (double(rl.c0) - (r - 1)) / dv - g.z_begin;
-            const int z0 = max(0, int(floor(zlo)) - 1);
-            const int z1 = min(g.Zs - 1, int(ceil(zhi)) + 1);
-            for (int z = z0; z <= z1; ++z) {
-                const float vi = row_at(rl, float(g.z_begin + z));
-                if (!row_ok(vi, g.vi_hi)) continue;
-                const int v0 = int(vi);
-                const float fv = __fsub_rn(vi, float(v0));
-                float bv;
-                if (v0 == r) bv = 1.0f - fv;
-                else if (v0 + 1 == r) bv = fv;
-                else continue;
-                acc += w * bu * bv * __ldg(&col[z]);
+        const int steps = __reduce_max_sync(kAll, cnt);
+        for (int st = 0; st < steps; ++st) {
+            // (2) this lane's candidate column for this step
+            bool hit = false;
+            float wb = 0.0f, mdv = 0.0f, c0 = 0.0f, inv = 0.0f;
+            int colidx = 0;
+            if (st < cnt) {
+                const int is = i0 + st;
+                const int x = x_major ? ip : is, y = x_major ? is : ip;
+                const float xw = world_coord(x, g.xPre, g.vs);
+                const float yw = world_coord(y, g.yPre, g.vs);
+                if (in_cylinder(xw, yw, g.r2)) {
+                    float U, u;
+                    column_geom(xw, yw, sn, cs, D, g.uOff, &U, &u);
+                    if (u >= g.lbU && u <= g.ubU) {
+                        const float ui = __fadd_rn(u, g.uPre);
+                        const int u0 = int(ui);
+                        const float fu = __fsub_rn(ui, float(u0));
+                        if (u0 == c || u0 + 1 == c) {
+                            hit = true;
+                            const float bu = u0 == c ? 1.0f - fu : fu;
+                            const float w = __fmul_rn(__fmul_rn(U, U), g.load_scale);
+                            wb = w * bu;
+                            const RowLine rl = row_line(U, h, g.zpv, g.vs, g.vPre);
+                            mdv = rl.mdv;
+                            c0 = rl.c0;
+                            inv = 1.0f / -rl.mdv;
+                            colidx = x * g.Y + y;
+                        }
+                    }
+                }
+            }
+            // (3) every lane adds the voxels of each hit column that reach its row
+            unsigned mask = __ballot_sync(kAll, hit);
+            while (mask) {
+                const int j = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const float jwb = __shfl_sync(kAll, wb, j);
+                const RowLine rl{__shfl_sync(kAll, mdv, j), __shfl_sync(kAll, c0, j)};
+                const float jinv = __shfl_sync(kAll, inv, j);
+                const int jcol = __shfl_sync(kAll, colidx, j);
+                // rows r-1 <= vi < r+1  <=>  z in ((c0-r-1)/dv, (c0-r+1)/dv], dv = -mdv > 0
+                // (box z; a margin of one slice on each side absorbs the rounding)
+                const float zlo = (rl.c0 - rf - 1.0f) * jinv, zhi = (rl.c0 - rf + 1.0f) * jinv;
+                const float zbig = float(g.z_begin + g.Zs) + 2.0f;
+                const int z0 = max(0, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) - 1 - g.z_begin);
+                const int z1 = min(g.Zs - 1, int(ceilf(fmaxf(fminf(zhi, zbig), -2.0f))) + 1 - g.z_begin);
+                const float* col = volz + (long long)jcol * g.Zs;
+                for (int z = z0; z <= z1; ++z) {
+                    const float vi = row_at(rl, float(g.z_begin + z));
+                    if (!row_ok(vi, g.vi_hi)) continue;
+                    const int v0 = int(vi);
+                    const float fv = __fsub_rn(vi, float(v0));
+                    float bv;
+                    if (v0 == r) bv = 1.0f - fv;
+                    else if (v0 + 1 == r) bv = fv;
+                    else continue;
+                    acc += jwb * bv * __ldg(&col[z]);
+                }
             }
         }
     }

@@ -23,6 +23,7 @@ class CtVolume:
         check(lib().ctb_create(ctypes.byref(self._ctx)))
         self._keep = None
         self._cb = None
+        self._pcb = None
         if csv_file is not None:
             self.sinogramFromImages(csv_file)
 
@@ -167,6 +168,29 @@ class CtVolume:
         out = np.empty((rows.value, cols.value), np.float32)
         self._ck(lib().ctb_get_cross_section(self._ctx, axis, index, out.ctypes.data, None, None))
         return out
+
+    def setCrossSectionAxis(self, axis: int):
+        self._ck(lib().ctb_set_cross_section_axis(self._ctx, int(axis)))
+
+    def setCrossSectionIndex(self, index: int):
+        self._ck(lib().ctb_set_cross_section_index(self._ctx, int(index)))
+
+    def _cs_info(self):
+        a, i, n = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._ck(lib().ctb_get_cross_section_info(self._ctx, ctypes.byref(a), ctypes.byref(i), ctypes.byref(n)))
+        return a.value, i.value, n.value
+
+    def getCrossSectionAxis(self): return self._cs_info()[0]
+    def getCrossSectionIndex(self): return self._cs_info()[1]
+    def getCrossSectionSize(self): return self._cs_info()[2]
+
+    def setPreviewCallback(self, fn):
+        """fn(percent, section) after every downloaded slab of reconstructVolume and once at 100 %;
+        section is a copy (rows x cols float32) of the current cross section."""
+        def tramp(pct, ptr, rows, cols, user):
+            fn(pct, np.ctypeslib.as_array(ptr, shape=(rows, cols)).copy())
+        self._pcb = L.PREVIEW_CB(tramp) if fn else L.PREVIEW_CB()
+        self._ck(lib().ctb_set_preview_callback(self._ctx, self._pcb, None))
 
     def stop(self):
         lib().ctb_stop(self._ctx)

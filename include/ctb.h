@@ -323,6 +323,25 @@ int ctb_load_volume(const char* raw_path, int x, int y, int z, int index_order, 
  * out holds rows*cols floats (row-major); rows/cols are returned. */
 int ctb_get_cross_section(const ctb_ctx* ctx, int axis, int index, float* out, int* rows, int* cols);
 
+/* Cross-section settings (setCrossSectionAxis / setCrossSectionIndex,
+ * Ct/CtVolume.cpp:395-429): changing the axis moves the index to the middle
+ * of the box along it; an index outside the box is ignored; loading a scan
+ * and changing the bounds re-centre or clamp it as the reference does
+ * (:317-326, :1411-1417). */
+int ctb_set_cross_section_axis(ctb_ctx* ctx, int axis);
+int ctb_set_cross_section_index(ctb_ctx* ctx, int index);
+/* getCrossSectionAxis / Index / Size (size = box extent along the axis). */
+int ctb_get_cross_section_info(const ctb_ctx* ctx, int* axis, int* index, int* size);
+/* Progress previews (reconstructionProgress / reconstructionFinished with the
+ * cross section, Ct/CtVolume.cpp:952, :1479-1483, :615): while
+ * ctb_reconstruct fills the context's own volume, cb receives the completion
+ * percentage and the current cross section (rows x cols floats, library-owned,
+ * valid during the call) after every downloaded z-slab, and once more at
+ * 100 % with the finished volume. Called from the reconstructing thread(s),
+ * one call at a time. */
+typedef void (*ctb_preview_cb)(double percent, const float* section, int rows, int cols, void* user);
+int ctb_set_preview_callback(ctb_ctx* ctx, ctb_preview_cb cb, void* user);
+
 /* ------------------------------------------------------ synthetic data */
 
 /* Analytic line integrals of a sum of ellipsoids (test phantoms), one value

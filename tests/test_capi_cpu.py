@@ -66,6 +66,26 @@ def test_csv_ingest_geometry(tmp_path, oracle):
     assert (g.x_from, g.x_to, g.z_from, g.z_to) == (int(0.25 * og.xSize + 0.5), int(0.75 * og.xSize + 0.5), 4, 8)
 
 
+def test_cross_section_settings(tmp_path):
+    """setCrossSectionAxis / Index and their re-centring (Ct/CtVolume.cpp:317-326, :395-429, :1411-1417)."""
+    from ct_b200 import AXIS_X, AXIS_Y, AXIS_Z
+    csv, imgs, geom = write_scan(tmp_path)
+    v = CtVolume(csv)
+    X, Y, Z = v.getXSize(), v.getYSize(), v.getZSize()
+    assert (v.getCrossSectionAxis(), v.getCrossSectionIndex(), v.getCrossSectionSize()) == (AXIS_Z, Z // 2, Z)
+    v.setCrossSectionAxis(AXIS_X)
+    assert (v.getCrossSectionIndex(), v.getCrossSectionSize()) == (X // 2, X)
+    v.setCrossSectionIndex(X - 1)
+    assert v.getCrossSectionIndex() == X - 1
+    v.setCrossSectionIndex(X)            # outside the box: ignored
+    assert v.getCrossSectionIndex() == X - 1
+    v.setVolumeBounds(0.0, 0.5, 0.0, 1.0, 0.0, 1.0)
+    g = v.grid()
+    assert v.getCrossSectionIndex() == (g.x_to - g.x_from) // 2   # clamped into the smaller box
+    v.setCrossSectionAxis(AXIS_Y)
+    assert v.getCrossSectionIndex() == Y // 2
+
+
 def test_csv_tiff_and_png_decoding(tmp_path):
     """Same pixels through PGM, TIFF (II and MM) and PNG give the same detector data."""
     import zlib, struct

@@ -341,3 +341,24 @@ def test_save_load_round_trip_and_cross_sections(tmp_path):
     assert np.array_equal(v.getVolumeCrossSection(2, Z // 2), zyx[Z // 2].T)             # rows x, cols y
     assert np.array_equal(v.getVolumeCrossSection(0, X // 3), zyx[::-1, :, X // 3])       # rows z (flipped), cols y
     assert np.array_equal(v.getVolumeCrossSection(1, Y // 2), zyx[::-1, Y // 2, ::-1])    # rows z (flipped), cols x (flipped)
+
+
+def test_progress_previews(tmp_path):
+    """Previews after every slab show the finished slabs and zeros elsewhere; the last one is the
+    finished volume's cross section (reconstructionProgress / reconstructionFinished)."""
+    csv, imgs, geom = c1_scan(tmp_path, n_views=40, W=64, H=64)
+    v = CtVolume(csv)
+    v.setSlabHeight(16)
+    v.setCrossSectionAxis(ct_b200.AXIS_Y)
+    seen = []
+    v.setPreviewCallback(lambda pct, sec: seen.append((pct, sec)))
+    v.reconstructVolume()
+    final = v.getVolumeCrossSection(ct_b200.AXIS_Y, v.getCrossSectionIndex())
+    Z = v.getZSize()
+    assert len(seen) >= Z // 16
+    assert seen[-1][0] == 100.0 and np.array_equal(seen[-1][1], final)
+    assert all(b[0] >= a[0] for a, b in zip(seen, seen[1:]))
+    # first preview (after slab 1 was issued): slab 0 finished, the rest still zero; rows run z = Z-1 .. 0
+    first = seen[0][1]
+    assert np.array_equal(first[Z - 16:], final[Z - 16:])
+    assert not first[:Z - 32].any()

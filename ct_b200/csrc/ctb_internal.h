@@ -100,12 +100,13 @@ ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, i
 // Backprojection of views [0, n) from `views` (device view table) into vol.
 // hmax bounds |height offset| (pixels) over the views. Dispatches to the
 // shared-memory (TMA) kernel when possible, else to the global-gather kernel.
+int bp_pick_zc(int slab_slices);
 int backproject_launch(const void* proj, int store_type, const float4* views, int n_views,
                        const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s);
 int backproject_global_launch(const void* proj, int store_type, const float4* views, int n_views,
                               const ProjGeom& g, float* vol, int accumulate, cudaStream_t s);
 // Returns CTB_ERR_UNSUPPORTED (nothing launched) when the geometry or layout
-// does not suit the TMA kernel. zc: z voxels per thread (8 or 16).
+// does not suit the TMA kernel. zc: z voxels per thread (8, 16 or 32).
 int backproject_tma_launch(const void* proj, int store_type, const float4* views, int n_views,
                            const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s,
                            int zc = 16);

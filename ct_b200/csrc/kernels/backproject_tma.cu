@@ -337,7 +337,7 @@ __device__ void pipe_abort_drain(Pipe<NBUF>& p, unsigned seq) {
 }
 
 template <typename T, int ZC, int NBUF>
-__global__ void __launch_bounds__(kThreads, 4) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(kThreads, ZC > 16 ? 3 : 4) bp_tma_kernel(const __grid_constant__ CUtensorMap map,
                                                           const T* __restrict__ proj,
                                                           const float4* __restrict__ views, int n_views,
                                                           ProjGeom g, Box bx, float* __restrict__ vol,
@@ -515,6 +515,7 @@ template <typename T>
 int launch_zc(const void* proj, const float4* views, int n_views, const ProjGeom& g, double hmax, float* vol,
               int accumulate, int zc, cudaStream_t s) {
     if (zc == 8) return launch_t<T, 8>((const T*)proj, views, n_views, g, hmax, vol, accumulate, s);
+    if (zc == 32) return launch_t<T, 32>((const T*)proj, views, n_views, g, hmax, vol, accumulate, s);
     return launch_t<T, 16>((const T*)proj, views, n_views, g, hmax, vol, accumulate, s);
 }
 

@@ -323,9 +323,28 @@ __global__ void __launch_bounds__(1024) filter_kernel(const InT* __restrict__ ra
             if (has1) out[obase + a.out_pitch + c] = to_store<OutT>(z.y * a.store_scale);
         }
     };
-    // preprocessing is kept out of the first FFT stage: done per element here
-    // it keeps the register footprint small (it involves log, sqrt and divide)
-    for (int c = lt; c < M; c += TG) s[c] = load(c);
+    // Preprocessing is kept out of the first FFT stage (done there it raises the
+    // register footprint: it involves log, sqrt and divide). All 16 raw loads of
+    // a thread (8 columns x 2 rows; TG = M/8) are issued before any arithmetic,
+    // so their latencies overlap instead of adding up.
+    InT v0[8], v1[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int c = lt + k * TG;
+        const bool in = active && c < W;
+        v0[k] = in ? raw[base0 + c] : InT(0);
+        v1[k] = in && has1 ? raw[base0 + W + c] : InT(0);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int c = lt + k * TG;
+        float2 z = make_float2(0.f, 0.f);
+        if (active && c < W) {
+            z.x = preprocess(raw_value(&v0[k], a), r0, c, a);
+            if (has1) z.y = preprocess(raw_value(&v1[k], a), r0 + 1, c, a);
+        }
+        s[c] = z;
+    }
     __syncthreads();
     fft_run<false, kFromSmem, kToSmemTimesK>(s, M, a.logM, tw, K, lt, TG, load, store);
     fft_run<true, kFromSmem, kToOutput>(s, M, a.logM, tw, K, lt, TG, load, store);

@@ -118,12 +118,14 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                 const RowLine rl{__shfl_sync(kAll, mdv, j), __shfl_sync(kAll, c0, j)};
                 const float jinv = __shfl_sync(kAll, inv, j);
                 const int jcol = __shfl_sync(kAll, colidx, j);
-                // rows r-1 <= vi < r+1  <=>  z in ((c0-r-1)/dv, (c0-r+1)/dv], dv = -mdv > 0
-                // (box z; a margin of one slice on each side absorbs the rounding)
-                const float zlo = (rl.c0 - rf - 1.0f) * jinv, zhi = (rl.c0 - rf + 1.0f) * jinv;
+                // rows r-1 <= vi < r+1  <=>  box z in ((c0-r-1)/dv, (c0-r+1)/dv], dv = -mdv > 0,
+                // widened by m for the rounding of vi, of the quotients and of 1/dv (together
+                // below inv/16 for rows under 2^17); the exact test below decides
+                const float m = 0.08f * jinv + 0.01f;
+                const float zlo = (rl.c0 - rf - 1.0f) * jinv - m, zhi = (rl.c0 - rf + 1.0f) * jinv + m;
                 const float zbig = float(g.z_begin + g.Zs) + 2.0f;
-                const int z0 = max(0, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) - 1 - g.z_begin);
-                const int z1 = min(g.Zs - 1, int(ceilf(fmaxf(fminf(zhi, zbig), -2.0f))) + 1 - g.z_begin);
+                const int z0 = max(0, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) + 1 - g.z_begin);
+                const int z1 = min(g.Zs - 1, int(floorf(fmaxf(fminf(zhi, zbig), -2.0f))) - g.z_begin);
                 const float* col = volz + (long long)jcol * g.Zs;
                 for (int z = z0; z <= z1; ++z) {
                     const float vi = row_at(rl, float(g.z_begin + z));

@@ -362,3 +362,27 @@ def test_progress_previews(tmp_path):
     first = seen[0][1]
     assert np.array_equal(first[Z - 16:], final[Z - 16:])
     assert not first[:Z - 32].any()
+
+
+@pytest.mark.parametrize("vs,uoff,heights", [(1.0, 0.0, False), (0.6, 1.5, True), (2.5, -2.0, False)])
+def test_forward_is_the_exact_transpose(vs, uoff, heights):
+    """Every matrix element: A e_voxel (forward projector) against A^T e_pixel (backprojector)."""
+    V, H, W, n = 3, 14, 16, 6
+    rng = np.random.default_rng(int(vs * 10))
+    det, _ = ops.detector(W, H, 40.0, u_offset=uoff)
+    grid = ops.custom_grid(det, (n, n, n), vs)
+    ang = rng.uniform(0, 360, V)
+    h = rng.uniform(-1.5, 1.5, V) if heights else None
+    A = np.zeros((V * H * W, n * n * n))
+    for k in range(n * n * n):
+        e = torch.zeros(n * n * n, device="cuda")
+        e[k] = 1.0
+        A[:, k] = ops.forward_project(e.view(n, n, n), ang, h, det, grid).cpu().numpy().ravel()
+    At = np.zeros((n * n * n, V * H * W))
+    for k in range(V * H * W):
+        e = torch.zeros(V * H * W, device="cuda")
+        e[k] = 1.0
+        At[:, k] = ops.backproject(e.view(V, H, W), ang, h, det, grid).cpu().numpy().ravel()
+    assert np.count_nonzero(A) > 100
+    assert np.array_equal(A != 0, At.T != 0)
+    np.testing.assert_allclose(A, At.T, rtol=1e-6, atol=1e-7)

@@ -539,7 +539,7 @@ def run_ours(args):
     bp_gups = units / (main["bp_ms"] * 1e-3) / 1e9
     bytes_px_in, bytes_px_out = 2, (2 if store != L.FP32 else 4)
     filt_gbs = V * H * W * (bytes_px_in + bytes_px_out) / (main["filter_ms"] * 1e-3) / 1e9
-    roofline = {"bound": "fetch", "kernel": "bp_kernel", "achieved": bp_gups, "peak": peak_gups, "unit": "GUPS",
+    roofline = {"bound": "fetch", "kernel": "bp_tma_kernel", "achieved": bp_gups, "peak": peak_gups, "unit": "GUPS",
                 "frac": bp_gups / peak_gups, "traffic": None,
                 "peak_basis": f"{sm_count} SMs x {clock_mhz:.0f} MHz (median sampled) x 32 lanes / 4 texel loads"}
     roofline_filter = {"bound": "hbm", "kernel": "filter_kernel", "achieved": filt_gbs, "peak": peaks["hbm_gbs"],

@@ -110,7 +110,7 @@ SIGNATURES = {
     "ctb_batch_create": (I, [P, I, P, I, P]),
     "ctb_batch_run": (I, [P, P]),
     "ctb_batch_run_sequential": (I, [P, P]),
-    "ctb_batch_tuning": (I, [P, P, P, P, P]),
+    "ctb_batch_tuning": (I, [P, P, P, P, P, P]),
     "ctb_batch_destroy": (None, [P]),
 }
 

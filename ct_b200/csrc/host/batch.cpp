@@ -29,7 +29,7 @@ struct ctb_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     int zc = 16;
-    double ms16 = -1, ms8 = -1;
+    double ms32 = -1, ms16 = -1, ms8 = -1;
 
     ~ctb_batch() {
         cudaSetDevice(device);
@@ -187,7 +187,7 @@ int ctb_batch_create(ctb_batch** out, int n, const ctb_scan* scans, int store_ty
     std::vector<double> times;
     int plan_err = CTB_OK;
     b->zc = Autotuner::instance().pick(
-        key, {16, 8},
+        key, {32, 16, 8},
         [&](int zc) -> double {
             BpBatchPlan plan;
             if (bp_batch_plan(store_type, zc, b->bp.data(), n, &plan) != CTB_OK) return -1.0;
@@ -209,7 +209,7 @@ int ctb_batch_create(ctb_batch** out, int n, const ctb_scan* scans, int store_ty
             return st == CTB_OK ? double(ms) : -1.0;
         },
         &times);
-    if (times.size() == 2) { b->ms16 = times[0]; b->ms8 = times[1]; }
+    if (times.size() == 3) { b->ms32 = times[0]; b->ms16 = times[1]; b->ms8 = times[2]; }
     int st = bp_batch_plan(store_type, b->zc, b->bp.data(), n, &b->plan);
     if (st != CTB_OK)
         return bail(fail("ctb_batch_create: a scan does not suit the persistent backprojector", plan_err ? plan_err : st));
@@ -257,9 +257,10 @@ int ctb_batch_run_sequential(ctb_batch* b, void* stream) {
     return CTB_OK;
 }
 
-int ctb_batch_tuning(const ctb_batch* b, int* zc, double* ms16, double* ms8, int* n_persistent) {
+int ctb_batch_tuning(const ctb_batch* b, int* zc, double* ms32, double* ms16, double* ms8, int* n_persistent) {
     if (!b) return ctb::fail("ctb_batch_tuning: invalid batch", CTB_ERR_ARG);
     if (zc) *zc = b->zc;
+    if (ms32) *ms32 = b->ms32;
     if (ms16) *ms16 = b->ms16;
     if (ms8) *ms8 = b->ms8;
     if (n_persistent) *n_persistent = int(b->plan.included.size());

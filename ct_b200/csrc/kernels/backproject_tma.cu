@@ -370,7 +370,7 @@ struct __align__(128) ScanDesc {
 };
 
 template <typename T, int ZC, int NBUF>
-__global__ void __launch_bounds__(kThreads, 4) bp_batch_kernel(const ScanDesc* __restrict__ scans, int n_scans,
+__global__ void __launch_bounds__(kThreads, ZC > 16 ? 3 : 4) bp_batch_kernel(const ScanDesc* __restrict__ scans, int n_scans,
                                                             const long long* __restrict__ tile_start,
                                                             unsigned long long* queue, int buf_stride) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -536,9 +536,9 @@ int batch_plan_t(const BpBatchScan* scans, int n, BpBatchPlan* plan) {
         ScanDesc d;
         std::memset(&d, 0, sizeof d);
         // The persistent kernel sizes its buffers for the largest box of the batch;
-        // a scan whose box would push it below four CTAs per SM (three buffers each)
-        // runs through its own launch instead.
-        constexpr size_t kBoxBudget = (227 * 1024 / 4 - 2048) / 3;
+        // a scan whose box would push it below its CTAs per SM (four, or three at
+        // 32 z voxels per thread; three buffers each) runs through its own launch.
+        constexpr size_t kBoxBudget = (227 * 1024 / (ZC > 16 ? 3 : 4) - 2048) / 3;
         if (!box_dims(sc.g, ZC, sc.hmax, sizeof(T), &d.bx) || size_t(d.bx.buf_elems) * sizeof(T) > kBoxBudget ||
             !make_map((const T*)sc.proj, sc.n_views, sc.g, d.bx, &d.map)) {
             plan->excluded.push_back(i);
@@ -581,6 +581,7 @@ int batch_plan_t(const BpBatchScan* scans, int n, BpBatchPlan* plan) {
 template <typename T>
 int batch_plan_zc(const BpBatchScan* scans, int n, int zc, BpBatchPlan* plan) {
     if (zc == 8) return batch_plan_t<T, 8>(scans, n, plan);
+    if (zc == 32) return batch_plan_t<T, 32>(scans, n, plan);
     return batch_plan_t<T, 16>(scans, n, plan);
 }
 
@@ -590,6 +591,14 @@ void batch_launch_t(const BpBatchPlan& plan, const void* desc, const long long* 
     auto kern = plan.nbuf == 3 ? bp_batch_kernel<T, ZC, 3> : bp_batch_kernel<T, ZC, 2>;
     kern<<<plan.grid, kThreads, plan.smem, s>>>(static_cast<const ScanDesc*>(desc), n, tile_start, queue,
                                                 plan.buf_stride);
+}
+
+template <typename T>
+void batch_launch_zc(const BpBatchPlan& plan, const void* desc, const long long* tile_start, int n,
+                     unsigned long long* queue, cudaStream_t s) {
+    if (plan.zc == 8) batch_launch_t<T, 8>(plan, desc, tile_start, n, queue, s);
+    else if (plan.zc == 32) batch_launch_t<T, 32>(plan, desc, tile_start, n, queue, s);
+    else batch_launch_t<T, 16>(plan, desc, tile_start, n, queue, s);
 }
 
 }  // namespace
@@ -608,7 +617,7 @@ int backproject_tma_launch(const void* proj, int store_type, const float4* views
 int bp_batch_plan(int store_type, int zc, const BpBatchScan* scans, int n, BpBatchPlan* plan) {
     if (n <= 0) return CTB_ERR_ARG;
     plan->store_type = store_type;
-    plan->zc = zc == 8 ? 8 : 16;
+    plan->zc = (zc == 8 || zc == 32) ? zc : 16;
     switch (store_type) {
         case CTB_FP32: return batch_plan_zc<float>(scans, n, plan->zc, plan);
         case CTB_FP16: return batch_plan_zc<__half>(scans, n, plan->zc, plan);
@@ -620,20 +629,10 @@ int bp_batch_plan(int store_type, int zc, const BpBatchScan* scans, int n, BpBat
 int bp_batch_launch(const BpBatchPlan& plan, const void* desc, const long long* tile_start, int n,
                     unsigned long long* queue, cudaStream_t s) {
     if (n <= 0) return CTB_OK;
-    const bool z8 = plan.zc == 8;
     switch (plan.store_type) {
-        case CTB_FP32:
-            z8 ? batch_launch_t<float, 8>(plan, desc, tile_start, n, queue, s)
-               : batch_launch_t<float, 16>(plan, desc, tile_start, n, queue, s);
-            break;
-        case CTB_FP16:
-            z8 ? batch_launch_t<__half, 8>(plan, desc, tile_start, n, queue, s)
-               : batch_launch_t<__half, 16>(plan, desc, tile_start, n, queue, s);
-            break;
-        case CTB_BF16:
-            z8 ? batch_launch_t<__nv_bfloat16, 8>(plan, desc, tile_start, n, queue, s)
-               : batch_launch_t<__nv_bfloat16, 16>(plan, desc, tile_start, n, queue, s);
-            break;
+        case CTB_FP32: batch_launch_zc<float>(plan, desc, tile_start, n, queue, s); break;
+        case CTB_FP16: batch_launch_zc<__half>(plan, desc, tile_start, n, queue, s); break;
+        case CTB_BF16: batch_launch_zc<__nv_bfloat16>(plan, desc, tile_start, n, queue, s); break;
         default: return CTB_ERR_ARG;
     }
     return cuda_status(cudaGetLastError(), "bp_batch_kernel launch");

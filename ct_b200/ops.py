@@ -151,9 +151,12 @@ class Batch:
         check(lib().ctb_batch_run_sequential(self._h, _stream(stream)))
 
     def tuning(self):
-        zc, a, b, n = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
-        check(lib().ctb_batch_tuning(self._h, ctypes.byref(zc), ctypes.byref(a), ctypes.byref(b), ctypes.byref(n)))
-        return {"zc": zc.value, "ms_zc16": a.value, "ms_zc8": b.value, "persistent_scans": n.value}
+        zc, n = ctypes.c_int(), ctypes.c_int()
+        t32, t16, t8 = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        check(lib().ctb_batch_tuning(self._h, ctypes.byref(zc), ctypes.byref(t32), ctypes.byref(t16), ctypes.byref(t8),
+                                     ctypes.byref(n)))
+        return {"zc": zc.value, "ms_zc32": t32.value, "ms_zc16": t16.value, "ms_zc8": t8.value,
+                "persistent_scans": n.value}
 
     def __del__(self):
         h = getattr(self, "_h", None)

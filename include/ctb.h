@@ -189,10 +189,12 @@ typedef struct ctb_batch ctb_batch;
 int ctb_batch_create(ctb_batch** batch, int n_scans, const ctb_scan* scans, int store_type, void* stream);
 int ctb_batch_run(ctb_batch* batch, void* stream);             /* replay the graph */
 int ctb_batch_run_sequential(ctb_batch* batch, void* stream);  /* scan by scan, separate launches */
-/* Autotuner outcome: chosen z voxels per thread, the timed candidates (ms, z = 16 and 8) and how
- * many scans the persistent kernel takes (scans with voxels so coarse that a tile's footprint box
- * exceeds the persistent kernel's shared-memory budget get their own launch inside the same graph). */
-int ctb_batch_tuning(const ctb_batch* batch, int* zc, double* ms_zc16, double* ms_zc8, int* n_persistent);
+/* Autotuner outcome: chosen z voxels per thread, the timed candidates (ms, z = 32, 16 and 8; -1
+ * where a candidate could not run) and how many scans the persistent kernel takes (scans with
+ * voxels so coarse that a tile's footprint box exceeds the persistent kernel's shared-memory
+ * budget get their own launch inside the same graph). */
+int ctb_batch_tuning(const ctb_batch* batch, int* zc, double* ms_zc32, double* ms_zc16, double* ms_zc8,
+                     int* n_persistent);
 void ctb_batch_destroy(ctb_batch* batch);
 
 /* ------------------------------------------------------ facade layer */

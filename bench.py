@@ -42,6 +42,11 @@ CONFIGS = {
 }
 FILTERS = {"ramlak": 0, "shepplogan": 1, "hann": 2}
 
+# DRAM bytes (read + write) of one backprojection launch per voxel-view update, from one
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of a C3 slab launch
+# (1024 x 1024 x 128 voxels x 1440 views of 2048^2, FP16): 138.7 GB / 1.93e11 updates
+BP_DRAM_BYTES_PER_UPDATE = {"c3": 138.72e9 / (1024 * 1024 * 128 * 1440)}
+
 
 # --------------------------------------------------------------------- clocks
 class ClockSampler:
@@ -540,7 +545,11 @@ def run_ours(args):
     bytes_px_in, bytes_px_out = 2, (2 if store != L.FP32 else 4)
     filt_gbs = V * H * W * (bytes_px_in + bytes_px_out) / (main["filter_ms"] * 1e-3) / 1e9
     roofline = {"bound": "fetch", "kernel": "bp_tma_kernel", "achieved": bp_gups, "peak": peak_gups, "unit": "GUPS",
-                "frac": bp_gups / peak_gups, "traffic": None,
+                "frac": bp_gups / peak_gups,
+                "traffic": (BP_DRAM_BYTES_PER_UPDATE[args.config] * X * Y * slab * V
+                            if args.config in BP_DRAM_BYTES_PER_UPDATE and args.store == "fp16" else None),
+                "traffic_unit": "DRAM bytes per backprojection launch (one slab)",
+                "algorithmic_bytes_per_launch": 8.0 * X * Y * slab * V,
                 "peak_basis": f"{sm_count} SMs x {clock_mhz:.0f} MHz (median sampled) x 32 lanes / 4 texel loads"}
     roofline_filter = {"bound": "hbm", "kernel": "filter_kernel", "achieved": filt_gbs, "peak": peaks["hbm_gbs"],
                        "unit": "GB/s", "frac": filt_gbs / peaks["hbm_gbs"], "peak_kind": peak_kind,

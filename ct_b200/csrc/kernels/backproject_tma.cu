@@ -128,12 +128,16 @@ __device__ __forceinline__ bool aborted(const volatile int* f) { return *f != 0;
 // One tile (32 x 8 columns x ZC voxels of one slab) over every view.
 // seq: box sequence number of this CTA (identical in all threads), advanced by
 // n_views when the tile loads boxes. Returns false if a bounded wait gave up.
+// rot: the tile visits the views in the order rot, rot + 1, ... (mod n_views);
+// tiles that start later start further on, so the CTAs resident at one time
+// read the same few views and share them in L2 (2.3x less DRAM traffic on a
+// 1024^3 slab of 1440 views of 2048^2).
 template <typename T, int ZC, int NBUF>
 __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __restrict__ proj,
                                           const float4* __restrict__ views, int n_views, const ProjGeom& g,
                                           const Box& bx, int buf_stride, float* __restrict__ vol, int accumulate,
                                           int tile_x, int tile_y, int tile_z, Pipe<NBUF>& p, T* buf,
-                                          unsigned& seq) {
+                                          unsigned& seq, int rot) {
     volatile int* abort_flag = &p.abort_flag;
     // Consumer warp w covers an 8 (x) x 4 (y) patch of columns: its lanes then
     // sample a compact patch of the box (a few rows x ~12 words), which keeps
@@ -190,7 +194,8 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
             // footprint of the whole ZC tile (voxels past the slab end are evaluated
             // too and dropped at the store): project the 4 (x, y) corners at both z ends
             float umin = 3.0e38f, umax = -3.0e38f, vmin = 3.0e38f, vmax = -3.0e38f;
-            const float4 q = __ldg(&views[iv]);
+            const int vv = rot ? (iv + rot) % n_views : iv;
+            const float4 q = __ldg(&views[vv]);
             if (lane < 4) {
                 const int cx = (lane & 1) ? x1 : x0;
                 const int cy = (lane >> 1) ? y1 : y0;
@@ -221,7 +226,7 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                 p.ovf[b] = (int(floorf(umax)) + 3 - uo > bx.BU) || (int(floorf(vmax)) + 3 - vo > bx.BV);
                 mbar_expect_tx(&p.full[b], uint32_t(bx.BU) * bx.BV * sizeof(T));
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                tma_load_3d(buf + size_t(b) * buf_stride, map, uo, vo, iv, &p.full[b]);
+                tma_load_3d(buf + size_t(b) * buf_stride, map, uo, vo, vv, &p.full[b]);
             }
             __syncwarp();
         }
@@ -341,14 +346,18 @@ __global__ void __launch_bounds__(kThreads, ZC > 16 ? 3 : 4) bp_tma_kernel(const
                                                           const T* __restrict__ proj,
                                                           const float4* __restrict__ views, int n_views,
                                                           ProjGeom g, Box bx, float* __restrict__ vol,
-                                                          int accumulate) {
+                                                          int accumulate, int resident) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(16) Pipe<NBUF> p;
     if (threadIdx.x == 0) pipe_init(p);
     __syncthreads();
     unsigned seq = 0;
+    // CTAs start in launch order as earlier ones finish: the k-th starts about
+    // k / resident of a tile's time after the first, so it starts that far on
+    const long long k = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
+    const int rot = int((k % resident) * n_views / resident);
     tile_pass<T, ZC, NBUF>(&map, proj, views, n_views, g, bx, bx.buf_elems, vol, accumulate, blockIdx.x,
-                           blockIdx.y, blockIdx.z, p, reinterpret_cast<T*>(smem_raw), seq);
+                           blockIdx.y, blockIdx.z, p, reinterpret_cast<T*>(smem_raw), seq, rot);
     __syncthreads();
     if (threadIdx.x == kConsumerWarps * 32 && p.abort_flag) pipe_abort_drain(p, seq);
 }
@@ -408,9 +417,10 @@ __global__ void __launch_bounds__(kThreads, ZC > 16 ? 3 : 4) bp_batch_kernel(con
         __syncthreads();
         if (p.item >= total || p.abort_flag) break;
         const ScanDesc& d = scans[s_scan];
+        const int rot = int((p.item % gridDim.x) * d.n_views / gridDim.x);
         tile_pass<T, ZC, NBUF>(&d.map, static_cast<const T*>(d.proj), d.views, d.n_views, sg, sbx, buf_stride,
                                d.vol, d.accumulate, s_tile[0], s_tile[1], s_tile[2], p,
-                               reinterpret_cast<T*>(smem_raw), seq);
+                               reinterpret_cast<T*>(smem_raw), seq, rot);
         __syncthreads();
     }
     if (threadIdx.x == kConsumerWarps * 32 && p.abort_flag) pipe_abort_drain(p, seq);
@@ -507,7 +517,11 @@ int launch_t(const T* proj, const float4* views, int n_views, const ProjGeom& g,
     CTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     dim3 grid((g.X + kTX - 1) / kTX, (g.Y + kTY - 1) / kTY, (g.Zs + ZC - 1) / ZC);
     if (grid.y > 65535 || grid.z > 65535) return CTB_ERR_UNSUPPORTED;
-    kern<<<grid, kThreads, smem, s>>>(map, proj, views, n_views, g, bx, vol, accumulate);
+    int per_sm = 0, dev = 0, sms = 0;
+    CTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
+    CTB_CUDA_TRY(cudaGetDevice(&dev));
+    CTB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    kern<<<grid, kThreads, smem, s>>>(map, proj, views, n_views, g, bx, vol, accumulate, std::max(1, per_sm * sms));
     return cuda_status(cudaGetLastError(), "bp_tma_kernel launch");
 }
 

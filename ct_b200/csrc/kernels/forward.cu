@@ -9,8 +9,8 @@
 // voxels with u0 in {c-1, c} and v0 in {r-1, r} of
 //     w * (u0 == c ? 1-fu : fu) * (v0 == r ? 1-fv : fv) * vol.
 //
-// Ray-driven gather (deterministic, no atomics). A warp owns 32 consecutive
-// detector rows of one detector column c of one view; everything that depends
+// Ray-driven gather (deterministic, no atomics). A warp owns 128 detector rows
+// (four per lane) of one detector column c of one view; everything that depends
 // only on (view, c) -- which voxel columns can reach c -- is shared by the
 // warp instead of being recomputed per lane:
 //  1. the warp walks the in-plane axis that is most perpendicular to the ray,
@@ -22,7 +22,8 @@
 //     discrete decisions u0, v0 and the masks agree bit for bit);
 //  3. the columns that reach c are broadcast one at a time (ballot + shuffles)
 //     and every lane adds the one to three voxels of that column whose rows
-//     fall on its own detector row r.
+//     fall on each of its four detector rows (r, r + 32, r + 64, r + 96), so
+//     the search and the broadcast serve 128 rows.
 // The volume is read in a z-fastest copy so that a warp's lanes (consecutive
 // rows -> consecutive z) read contiguous memory.
 
@@ -33,14 +34,15 @@ namespace ctb {
 
 namespace {
 
-constexpr int kFR = 32, kFC = 8;
+// a CTA: kFC detector columns (one warp each) x kFR * kRPL rows (kRPL per lane)
+constexpr int kFR = 32, kFC = 8, kRPL = 4;
 constexpr unsigned kAll = 0xffffffffu;
 
 __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__ volz,
                                                        const float4* __restrict__ views, ProjGeom g,
                                                        float* __restrict__ proj, int accumulate) {
     const int lane = threadIdx.x;
-    const int r = blockIdx.x * kFR + lane;
+    const int r = blockIdx.x * (kFR * kRPL) + lane;  // rows r, r + 32, r + 64, r + 96
     const int c = blockIdx.y * kFC + threadIdx.y;
     const int iv = blockIdx.z;
     if (c >= g.W) return;  // whole warps leave together
@@ -53,8 +55,9 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
     const int ns = x_major ? g.Y : g.X;
     const float ppre = x_major ? g.xPre : g.yPre;
     const float spre = x_major ? g.yPre : g.xPre;
-    const float rf = float(r);
-    float acc = 0.0f;
+    float acc[kRPL];
+#pragma unroll
+    for (int k = 0; k < kRPL; ++k) acc[k] = 0.0f;
     for (int ip0 = 0; ip0 < np; ip0 += 32) {
         // (1) candidate range of this lane's position
         const int ip = ip0 + lane;
@@ -122,28 +125,37 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                 // widened by m for the rounding of vi, of the quotients and of 1/dv (together
                 // below inv/16 for rows under 2^17); the exact test below decides
                 const float m = 0.08f * jinv + 0.01f;
-                const float zlo = (rl.c0 - rf - 1.0f) * jinv - m, zhi = (rl.c0 - rf + 1.0f) * jinv + m;
                 const float zbig = float(g.z_begin + g.Zs) + 2.0f;
-                const int z0 = max(0, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) + 1 - g.z_begin);
-                const int z1 = min(g.Zs - 1, int(floorf(fmaxf(fminf(zhi, zbig), -2.0f))) - g.z_begin);
                 const float* col = volz + (long long)jcol * g.Zs;
-                for (int z = z0; z <= z1; ++z) {
-                    const float vi = row_at(rl, float(g.z_begin + z));
-                    if (!row_ok(vi, g.vi_hi)) continue;
-                    const int v0 = int(vi);
-                    const float fv = __fsub_rn(vi, float(v0));
-                    float bv;
-                    if (v0 == r) bv = 1.0f - fv;
-                    else if (v0 + 1 == r) bv = fv;
-                    else continue;
-                    acc += jwb * bv * __ldg(&col[z]);
+#pragma unroll
+                for (int k = 0; k < kRPL; ++k) {
+                    const int rk = r + k * kFR;
+                    const float rf = float(rk);
+                    const float zlo = (rl.c0 - rf - 1.0f) * jinv - m, zhi = (rl.c0 - rf + 1.0f) * jinv + m;
+                    const int z0 = max(0, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) + 1 - g.z_begin);
+                    const int z1 = min(g.Zs - 1, int(floorf(fmaxf(fminf(zhi, zbig), -2.0f))) - g.z_begin);
+                    for (int z = z0; z <= z1; ++z) {
+                        const float vi = row_at(rl, float(g.z_begin + z));
+                        if (!row_ok(vi, g.vi_hi)) continue;
+                        const int v0 = int(vi);
+                        const float fv = __fsub_rn(vi, float(v0));
+                        float bv;
+                        if (v0 == rk) bv = 1.0f - fv;
+                        else if (v0 + 1 == rk) bv = fv;
+                        else continue;
+                        acc[k] += jwb * bv * __ldg(&col[z]);
+                    }
                 }
             }
         }
     }
-    if (r >= g.H) return;
-    float* out = proj + (long long)iv * g.view_stride + (long long)r * g.W + c;
-    *out = accumulate ? (*out + acc) : acc;
+#pragma unroll
+    for (int k = 0; k < kRPL; ++k) {
+        const int rk = r + k * kFR;
+        if (rk >= g.H) break;
+        float* out = proj + (long long)iv * g.view_stride + (long long)rk * g.W + c;
+        *out = accumulate ? (*out + acc[k]) : acc[k];
+    }
 }
 
 }  // namespace
@@ -162,7 +174,7 @@ int forward_launch(const float* vol, const float4* views, int n_views, const Pro
     int st = layout_launch(vol, g.X, g.Y, g.Zs, CTB_Z_FASTEST, CTB_LITTLE_ENDIAN, volz, s);
     if (st == CTB_OK) {
         dim3 block(kFR, kFC, 1);
-        dim3 grid((g.H + kFR - 1) / kFR, (g.W + kFC - 1) / kFC, n_views);
+        dim3 grid((g.H + kFR * kRPL - 1) / (kFR * kRPL), (g.W + kFC - 1) / kFC, n_views);
         fp_kernel<<<grid, block, 0, s>>>(volz, views, g, proj, accumulate);
         st = cuda_status(cudaGetLastError(), "fp_kernel launch");
     }

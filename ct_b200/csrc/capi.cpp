@@ -141,6 +141,25 @@ int ctb_backproject(const void* filtered, int store_type, int n_views, const dou
     return st;
 }
 
+int ctb_device_wait_timeouts(int device, unsigned* count, int reset) {
+    if (!count) return arg_error("null pointer");
+    int prev = 0;
+    CTB_CUDA_TRY(cudaGetDevice(&prev));
+    CTB_CUDA_TRY(cudaSetDevice(device));
+    const int st = ctb::device_wait_timeouts(count, reset);
+    cudaSetDevice(prev);
+    return st;
+}
+
+int ctb_diag_bounded_wait(int device, unsigned limit) {
+    int prev = 0;
+    CTB_CUDA_TRY(cudaGetDevice(&prev));
+    CTB_CUDA_TRY(cudaSetDevice(device));
+    const int st = ctb::bounded_wait_probe_run(limit, nullptr);
+    cudaSetDevice(prev);
+    return st;
+}
+
 int ctb_forward_project(const float* vol, const double* angles_deg, const double* height_offsets_px, int n_views,
                         const ctb_detector* det, const ctb_grid* grid, int z_begin, int z_end, float* proj,
                         int accumulate, void* stream) {

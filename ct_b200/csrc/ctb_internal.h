@@ -61,7 +61,17 @@ struct FilterArgs {
     float D, uPre, vPre;            // Feldkamp weight
     float store_scale;
     int out_pitch;                  // elements per filtered row (>= W; padding is left untouched)
+    // optional table (device): the Feldkamp weight of every detector pixel;
+    // null -> evaluated per pixel
+    const float* wt = nullptr;
 };
+
+// Build that table (exactly the per-pixel operations, evaluated once).
+int build_weight_table(const FilterArgs& a, float* t, cudaStream_t s);
+// Process-wide cache of weight tables per device and geometry. With build = 0
+// (inside a stream capture) only an existing table is returned; a missing one
+// stays null and the filter evaluates the weight per pixel.
+int pre_tables(FilterArgs* a, cudaStream_t s, bool build);
 
 // Launch the fused load/log/weight/FFT/window/IFFT/store kernel over n_views.
 int filter_launch(const void* raw, int raw_type, void* out, int store_type, const FilterArgs& a,
@@ -140,6 +150,9 @@ int bp_batch_launch(const BpBatchPlan& plan, const void* desc, const long long* 
                     unsigned long long* queue, cudaStream_t s);
 // Number of CTAs whose bounded mbarrier waits gave up since the last reset.
 int device_wait_timeouts(unsigned* count, int reset);
+// Run a wait that can never complete with the given try limit (diagnostic of
+// the bounded-wait path): CTB_ERR_TIMEOUT when it gave up, as it must.
+int bounded_wait_probe_run(unsigned limit, cudaStream_t s);
 
 int forward_launch(const float* vol, const float4* views, int n_views, const ProjGeom& g, float* proj,
                    int accumulate, cudaStream_t s);

@@ -138,6 +138,10 @@ int ctb_batch_create(ctb_batch** out, int n, const ctb_scan* scans, int store_ty
         int st = filter_tables(sc.det.width, sc.pad, sc.filter, s, &t);
         if (st != CTB_OK) return bail(st);
         b->tables.push_back(t);
+        // preprocessing tables now: the filters are captured into a graph later
+        FilterArgs pa = filter_args(sc.det, sc.raw_type, t.M, t.logM, sc.n_views, 1.0f);
+        st = pre_tables(&pa, s, true);
+        if (st != CTB_OK) return bail(st);
         // view table (FP64 geometry kernel)
         float4* v = nullptr;
         double* tmp = nullptr;

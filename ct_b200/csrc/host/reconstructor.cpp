@@ -854,6 +854,12 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     if (cudaStreamSynchronize(w.s_down) != cudaSuccess || cudaStreamSynchronize(w.s_comp) != cudaSuccess ||
         cudaStreamSynchronize(w.s_copy) != cudaSuccess)
         return cuda_fail("reconstruction");
+    unsigned gave_up = 0;
+    if (device_wait_timeouts(&gave_up, 1) == CTB_OK && gave_up) {
+        cleanup();
+        return fail(CTB_ERR_TIMEOUT, "A device wait of the backprojection gave up (" + std::to_string(gave_up) +
+                                         " times); the volume is incomplete.");
+    }
     float phase_ms = 0, tail_ms = 0;
     double f_ms = 0, b_ms = 0;
     cudaEventElapsedTime(&phase_ms, e_f0, e_f1);

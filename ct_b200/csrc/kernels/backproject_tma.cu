@@ -652,6 +652,49 @@ int bp_batch_launch(const BpBatchPlan& plan, const void* desc, const long long* 
     return cuda_status(cudaGetLastError(), "bp_batch_kernel launch");
 }
 
+namespace {
+// Diagnostic: a barrier initialised for two arrivals that only ever gets one,
+// waited on by a warp with the backprojector's bounded loop and the given
+// limit. The wait must give up; it records that as the backprojector does.
+__global__ void bounded_wait_probe(unsigned limit, int* gave_up) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 2);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&bar)) : "memory");
+    unsigned tries = 0;
+    bool done = false;
+    while (!(done = mbar_try_wait(&bar, 0)) && ++tries <= limit) {
+    }
+    if (!done && threadIdx.x == 0) {
+        atomicAdd(&g_wait_timeouts, 1u);
+        *gave_up = 1;
+    }
+}
+}  // namespace
+
+int bounded_wait_probe_run(unsigned limit, cudaStream_t s) {
+    int* d = nullptr;
+    CTB_CUDA_TRY(cudaMallocAsync((void**)&d, sizeof(int), s));
+    int st = cuda_status(cudaMemsetAsync(d, 0, sizeof(int), s), "probe flag");
+    if (st == CTB_OK) {
+        bounded_wait_probe<<<1, 32, 0, s>>>(limit, d);
+        st = cuda_status(cudaGetLastError(), "bounded_wait_probe launch");
+    }
+    int h = 0;
+    if (st == CTB_OK) st = cuda_status(cudaMemcpyAsync(&h, d, sizeof(int), cudaMemcpyDeviceToHost, s), "probe read");
+    if (st == CTB_OK) st = cuda_status(cudaStreamSynchronize(s), "probe");
+    cudaFreeAsync(d, s);
+    if (st != CTB_OK) return st;
+    if (h) {
+        set_global_error("a bounded device wait gave up after " + std::to_string(limit) + " tries");
+        return CTB_ERR_TIMEOUT;
+    }
+    return CTB_OK;
+}
+
 int device_wait_timeouts(unsigned* count, int reset) {
     CTB_CUDA_TRY(cudaMemcpyFromSymbol(count, g_wait_timeouts, sizeof(unsigned)));
     if (reset && *count) {

@@ -25,6 +25,7 @@
 // with two barriers per stage. Raw pixels are read once, filtered values are
 // written once: HBM traffic is the algorithmic minimum.
 
+#include <type_traits>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -134,13 +135,20 @@ template <> __device__ __forceinline__ float raw_value<float>(const float* p, co
 }
 
 // -ln(s * scale) * D / sqrt(D^2 + u^2 + v^2), no contraction (reference order).
-__device__ __forceinline__ float preprocess(float s, int r, int c, const FilterArgs& a) {
-    const float p = -logf(__fmul_rn(s, a.log_scale));
+__device__ __forceinline__ float log_part(float s, const FilterArgs& a) { return -logf(__fmul_rn(s, a.log_scale)); }
+__device__ __forceinline__ float weight_part(int r, int c, const FilterArgs& a) {
     const float u = __fsub_rn(float(c), a.uPre);
     const float v = __fadd_rn(-float(r), a.vPre);
     const float d2 = __fadd_rn(__fadd_rn(__fmul_rn(a.D, a.D), __fmul_rn(u, u)), __fmul_rn(v, v));
-    return __fmul_rn(p, __fdiv_rn(a.D, __fsqrt_rn(d2)));
+    return __fdiv_rn(a.D, __fsqrt_rn(d2));
 }
+__device__ __forceinline__ float preprocess(float s, int r, int c, const FilterArgs& a) {
+    return __fmul_rn(log_part(s, a), weight_part(r, c, a));
+}
+
+// TAB: the Feldkamp weight of every pixel comes from a table (exactly
+// weight_part's values), loaded together with the raw samples, instead of a
+// square root and a divide per pixel.
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -288,7 +296,7 @@ __device__ void fft_run(float2* s, int M, int logM, const float2* __restrict__ t
 }
 
 // One group of TG = M/8 threads per detector row pair; groups = blockDim/TG.
-template <typename InT, typename OutT>
+template <typename InT, typename OutT, bool TAB>
 __global__ void __launch_bounds__(1024) filter_kernel(const InT* __restrict__ raw, OutT* __restrict__ out,
                                                       FilterArgs a, const float2* __restrict__ tw,
                                                       const float* __restrict__ K) {
@@ -328,20 +336,29 @@ __global__ void __launch_bounds__(1024) filter_kernel(const InT* __restrict__ ra
     // a thread (8 columns x 2 rows; TG = M/8) are issued before any arithmetic,
     // so their latencies overlap instead of adding up.
     InT v0[8], v1[8];
+    float w0[8], w1[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int c = lt + k * TG;
         const bool in = active && c < W;
         v0[k] = in ? raw[base0 + c] : InT(0);
         v1[k] = in && has1 ? raw[base0 + W + c] : InT(0);
+        if constexpr (TAB) {
+            w0[k] = in ? __ldg(&a.wt[(size_t)r0 * W + c]) : 0.0f;
+            w1[k] = in && has1 ? __ldg(&a.wt[(size_t)(r0 + 1) * W + c]) : 0.0f;
+        }
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
         const int c = lt + k * TG;
         float2 z = make_float2(0.f, 0.f);
         if (active && c < W) {
-            z.x = preprocess(raw_value(&v0[k], a), r0, c, a);
-            if (has1) z.y = preprocess(raw_value(&v1[k], a), r0 + 1, c, a);
+            const float wa = TAB ? w0[k] : weight_part(r0, c, a);
+            z.x = __fmul_rn(log_part(raw_value(&v0[k], a), a), wa);
+            if (has1) {
+                const float wb = TAB ? w1[k] : weight_part(r0 + 1, c, a);
+                z.y = __fmul_rn(log_part(raw_value(&v1[k], a), a), wb);
+            }
         }
         s[c] = z;
     }
@@ -364,7 +381,8 @@ int launch_typed(const InT* raw, OutT* out, const FilterArgs& a, const float2* t
         set_global_error("filter: too many rows for one launch");
         return CTB_ERR_UNSUPPORTED;
     }
-    auto kern = filter_kernel<InT, OutT>;
+    const bool tab = a.wt != nullptr;
+    auto kern = tab ? filter_kernel<InT, OutT, true> : filter_kernel<InT, OutT, false>;
     if (smem > 48 * 1024)
         CTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
     kern<<<unsigned(blocks), threads, smem, s>>>(raw, out, a, tw, K);
@@ -433,8 +451,30 @@ FilterArgs filter_args(const ctb_detector& det, int raw_type, int M, int logM, l
     return a;
 }
 
-int filter_launch(const void* raw, int raw_type, void* out, int store_type, const FilterArgs& a,
+namespace {
+__global__ void weight_table_kernel(float* t, FilterArgs a) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int r = blockIdx.y;
+    if (c >= a.W) return;
+    t[(size_t)r * a.W + c] = weight_part(r, c, a);
+}
+}  // namespace
+
+int build_weight_table(const FilterArgs& a, float* t, cudaStream_t s) {
+    if (a.H > 65535) return CTB_ERR_UNSUPPORTED;
+    weight_table_kernel<<<dim3((a.W + 255) / 256, a.H), 256, 0, s>>>(t, a);
+    return cuda_status(cudaGetLastError(), "weight_table_kernel launch");
+}
+
+int filter_launch(const void* raw, int raw_type, void* out, int store_type, const FilterArgs& args,
                   const float2* tw, const float* K, cudaStream_t s) {
+    FilterArgs a = args;
+    if (!a.wt) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) cudaGetLastError();
+        const int st = pre_tables(&a, s, cs == cudaStreamCaptureStatusNone);
+        if (st != CTB_OK) return st;
+    }
     switch (raw_type) {
         case CTB_U8: return launch_out((const uint8_t*)raw, out, store_type, a, tw, K, s);
         case CTB_U16: return launch_out((const uint16_t*)raw, out, store_type, a, tw, K, s);

@@ -297,6 +297,20 @@ typedef struct {
 } ctb_timings;
 int ctb_get_timings(const ctb_ctx* ctx, ctb_timings* t);
 
+/* --------------------------------------------------- device waits */
+
+/* Every wait inside the backprojection kernels (for a box load, for a free
+ * buffer) is bounded; a wait that gives up makes its tile stop, leaves that
+ * part of the volume incomplete and is counted here. Returns the count on
+ * `device` since the last reset (reset != 0 clears it). ctb_reconstruct checks
+ * it and fails with CTB_ERR_TIMEOUT; callers of ctb_backproject check it after
+ * synchronising. No reference counterpart. */
+int ctb_device_wait_timeouts(int device, unsigned* count, int reset);
+/* Diagnostic of that path: one warp waits on a barrier that can never
+ * complete, with at most `limit` tries, and must give up: returns
+ * CTB_ERR_TIMEOUT (and adds 1 to the count) with the device still usable. */
+int ctb_diag_bounded_wait(int device, unsigned limit);
+
 /* ------------------------------------------------------ volume files */
 
 /* DataType, Common/types.h:27-36 (same order). */

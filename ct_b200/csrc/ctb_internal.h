@@ -25,6 +25,12 @@ int cuda_status(cudaError_t e, const char* what);
         if (_st != CTB_OK) return _st;                          \
     } while (0)
 
+// Raise a kernel's dynamic shared-memory allowance on the current device to
+// at least `bytes`. The attribute is per device and shared by all host
+// threads, so it is only ever raised: a launch prepared by one thread is never
+// invalidated by another thread lowering it.
+int ensure_dynamic_smem(const void* kernel, size_t bytes);
+
 inline size_t store_bytes(int store_type) { return store_type == CTB_FP32 ? 4 : 2; }
 inline size_t raw_bytes(int raw_type) { return raw_type == CTB_U8 ? 1 : raw_type == CTB_U16 ? 2 : 4; }
 

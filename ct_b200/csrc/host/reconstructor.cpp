@@ -719,8 +719,10 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     auto cuda_fail = [&](const char* what) {
         cudaStreamSynchronize(w.s_copy); cudaStreamSynchronize(w.s_comp); cudaStreamSynchronize(w.s_down);
         cleanup();
+        // the launch helpers record their own message when the CUDA error was
+        // already taken (or when a launch was refused without one)
         const cudaError_t e = cudaGetLastError();
-        return fail(CTB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+        return fail(CTB_ERR_CUDA, std::string(what) + ": " + (e != cudaSuccess ? cudaGetErrorString(e) : global_error()));
     };
 
     // ---- geometry tables (FP64 kernels)

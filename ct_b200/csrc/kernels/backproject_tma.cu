@@ -514,7 +514,7 @@ int launch_t(const T* proj, const float4* views, int n_views, const ProjGeom& g,
     const size_t smem = size_t(nbuf) * per_buf;
     if (smem > 200 * 1024) return CTB_ERR_UNSUPPORTED;
     auto kern = nbuf == 3 ? bp_tma_kernel<T, ZC, 3> : bp_tma_kernel<T, ZC, 2>;
-    CTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    if (const int st = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return st;
     dim3 grid((g.X + kTX - 1) / kTX, (g.Y + kTY - 1) / kTY, (g.Zs + ZC - 1) / ZC);
     if (grid.y > 65535 || grid.z > 65535) return CTB_ERR_UNSUPPORTED;
     int per_sm = 0, dev = 0, sms = 0;
@@ -583,7 +583,7 @@ int batch_plan_t(const BpBatchScan* scans, int n, BpBatchPlan* plan) {
     plan->smem = size_t(plan->nbuf) * per_buf;
     if (plan->smem > 200 * 1024) return CTB_ERR_UNSUPPORTED;
     auto kern = plan->nbuf == 3 ? bp_batch_kernel<T, ZC, 3> : bp_batch_kernel<T, ZC, 2>;
-    CTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(plan->smem)));
+    if (const int st = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), plan->smem)) return st;
     int per_sm = 0, dev = 0, sms = 0;
     CTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, plan->smem));
     CTB_CUDA_TRY(cudaGetDevice(&dev));

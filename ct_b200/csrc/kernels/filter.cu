@@ -384,7 +384,7 @@ int launch_typed(const InT* raw, OutT* out, const FilterArgs& a, const float2* t
     const bool tab = a.wt != nullptr;
     auto kern = tab ? filter_kernel<InT, OutT, true> : filter_kernel<InT, OutT, false>;
     if (smem > 48 * 1024)
-        CTB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+        if (const int st = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return st;
     kern<<<unsigned(blocks), threads, smem, s>>>(raw, out, a, tw, K);
     return cuda_status(cudaGetLastError(), "filter_kernel launch");
 }

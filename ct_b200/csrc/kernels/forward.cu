@@ -20,10 +20,12 @@
 //  2. step by step through those ranges, each lane evaluates one candidate
 //     column with the very same FP32 expressions as the backprojector (so the
 //     discrete decisions u0, v0 and the masks agree bit for bit);
-//  3. the columns that reach c are broadcast one at a time (ballot + shuffles)
-//     and every lane adds the one to three voxels of that column whose rows
-//     fall on each of its four detector rows (r, r + 32, r + 64, r + 96), so
-//     the search and the broadcast serve 128 rows.
+//  3. the columns that reach c are broadcast one at a time (ballot + shuffles);
+//     the lanes then walk that column's slices whose rows reach the warp's 128
+//     rows, one slice each, and add each slice's two row weights into the
+//     warp's row accumulators in shared memory. Lanes that write in the same
+//     instruction hold slices far enough apart that their rows differ, and the
+//     order of the additions is fixed, so the result is deterministic.
 // The volume is read in a z-fastest copy so that a warp's lanes (consecutive
 // rows -> consecutive z) read contiguous memory.
 
@@ -41,9 +43,11 @@ constexpr unsigned kAll = 0xffffffffu;
 __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__ volz,
                                                        const float4* __restrict__ views, ProjGeom g,
                                                        float* __restrict__ proj, int accumulate) {
+    __shared__ float s_rows[kFC][kFR * kRPL];  // per warp: rows R .. R + 127
     const int lane = threadIdx.x;
-    const int r = blockIdx.x * (kFR * kRPL) + lane;  // rows r, r + 32, r + 64, r + 96
+    const int R = blockIdx.x * (kFR * kRPL);  // first row of the warp
     const int c = blockIdx.y * kFC + threadIdx.y;
+    float* srow = s_rows[threadIdx.y];
     const int iv = blockIdx.z;
     if (c >= g.W) return;  // whole warps leave together
     const float4 q = __ldg(&views[iv]);
@@ -55,9 +59,9 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
     const int ns = x_major ? g.Y : g.X;
     const float ppre = x_major ? g.xPre : g.yPre;
     const float spre = x_major ? g.yPre : g.xPre;
-    float acc[kRPL];
 #pragma unroll
-    for (int k = 0; k < kRPL; ++k) acc[k] = 0.0f;
+    for (int k = 0; k < kRPL; ++k) srow[lane + k * kFR] = 0.0f;
+    __syncwarp();
     for (int ip0 = 0; ip0 < np; ip0 += 32) {
         // (1) candidate range of this lane's position
         const int ip = ip0 + lane;
@@ -121,40 +125,55 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                 const RowLine rl{__shfl_sync(kAll, mdv, j), __shfl_sync(kAll, c0, j)};
                 const float jinv = __shfl_sync(kAll, inv, j);
                 const int jcol = __shfl_sync(kAll, colidx, j);
-                // rows r-1 <= vi < r+1  <=>  box z in ((c0-r-1)/dv, (c0-r+1)/dv], dv = -mdv > 0,
-                // widened by m for the rounding of vi, of the quotients and of 1/dv (together
-                // below inv/16 for rows under 2^17); the exact test below decides
+                // slices whose rows can reach R-1 .. R+127: box z in
+                // ((c0-R-129)/dv, (c0-R+1)/dv], dv = -mdv > 0, widened by m for the
+                // rounding of vi, of the quotients and of 1/dv (together below inv/16
+                // for rows under 2^17); the exact row test below decides
                 const float m = 0.08f * jinv + 0.01f;
                 const float zbig = float(g.z_begin + g.Zs) + 2.0f;
+                const float zlo = (rl.c0 - float(R + kFR * kRPL) - 1.0f) * jinv - m;
+                const float zhi = (rl.c0 - float(R) + 1.0f) * jinv + m;
+                const int z0 = max(0, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) + 1 - g.z_begin);
+                const int z1 = min(g.Zs - 1, int(floorf(fmaxf(fminf(zhi, zbig), -2.0f))) - g.z_begin);
+                // lanes st slices apart: their rows differ by st * dv > 1.02, more than
+                // the rounding of two row coordinates (2^-6 for rows under 2^17), so
+                // the lanes of one instruction never share a row (at st >= Zs only
+                // lane 0 has a slice, so the cap keeps that true)
+                const int st = min(int(fminf(jinv, 1.0e7f) * 1.02f) + 1, max(1, g.Zs));
                 const float* col = volz + (long long)jcol * g.Zs;
-#pragma unroll
-                for (int k = 0; k < kRPL; ++k) {
-                    const int rk = r + k * kFR;
-                    const float rf = float(rk);
-                    const float zlo = (rl.c0 - rf - 1.0f) * jinv - m, zhi = (rl.c0 - rf + 1.0f) * jinv + m;
-                    const int z0 = max(0, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) + 1 - g.z_begin);
-                    const int z1 = min(g.Zs - 1, int(floorf(fmaxf(fminf(zhi, zbig), -2.0f))) - g.z_begin);
-                    for (int z = z0; z <= z1; ++z) {
-                        const float vi = row_at(rl, float(g.z_begin + z));
-                        if (!row_ok(vi, g.vi_hi)) continue;
-                        const int v0 = int(vi);
-                        const float fv = __fsub_rn(vi, float(v0));
-                        float bv;
-                        if (v0 == rk) bv = 1.0f - fv;
-                        else if (v0 + 1 == rk) bv = fv;
-                        else continue;
-                        acc[k] += jwb * bv * __ldg(&col[z]);
+                for (int zb = z0; zb <= z1; zb += kFR * st) {
+                    for (int q = 0; q < st; ++q) {
+                        const int z = zb + q + lane * st;
+                        int lr = -2;
+                        float ca = 0.0f, cb = 0.0f;
+                        if (z <= z1) {
+                            const float vi = row_at(rl, float(g.z_begin + z));
+                            if (row_ok(vi, g.vi_hi)) {
+                                const int v0 = int(vi);
+                                const float fv = __fsub_rn(vi, float(v0));
+                                const float val = jwb * __ldg(&col[z]);
+                                lr = v0 - R;
+                                ca = (1.0f - fv) * val;  // to row v0
+                                cb = fv * val;           // to row v0 + 1
+                            }
+                        }
+                        if (lr >= 0 && lr < kFR * kRPL) srow[lr] += ca;
+                        __syncwarp();
+                        if (lr + 1 >= 0 && lr + 1 < kFR * kRPL) srow[lr + 1] += cb;
+                        __syncwarp();
                     }
                 }
             }
         }
     }
+    __syncwarp();
 #pragma unroll
     for (int k = 0; k < kRPL; ++k) {
-        const int rk = r + k * kFR;
+        const int rk = R + lane + k * kFR;
         if (rk >= g.H) break;
         float* out = proj + (long long)iv * g.view_stride + (long long)rk * g.W + c;
-        *out = accumulate ? (*out + acc[k]) : acc[k];
+        const float acc = srow[lane + k * kFR];
+        *out = accumulate ? (*out + acc) : acc;
     }
 }
 

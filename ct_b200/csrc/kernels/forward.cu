@@ -9,8 +9,8 @@
 // voxels with u0 in {c-1, c} and v0 in {r-1, r} of
 //     w * (u0 == c ? 1-fu : fu) * (v0 == r ? 1-fv : fv) * vol.
 //
-// Ray-driven gather (deterministic, no atomics). A warp owns 128 detector rows
-// (four per lane) of one detector column c of one view; everything that depends
+// Ray-driven gather (deterministic, no atomics). A warp owns 256 detector rows
+// (eight per lane) of one detector column c of one view; everything that depends
 // only on (view, c) -- which voxel columns can reach c -- is shared by the
 // warp instead of being recomputed per lane:
 //  1. the warp walks the in-plane axis that is most perpendicular to the ray,
@@ -21,7 +21,7 @@
 //     column with the very same FP32 expressions as the backprojector (so the
 //     discrete decisions u0, v0 and the masks agree bit for bit);
 //  3. the columns that reach c are broadcast one at a time (ballot + shuffles);
-//     the lanes then walk that column's slices whose rows reach the warp's 128
+//     the lanes then walk that column's slices whose rows reach the warp's 256
 //     rows, one slice each, and add each slice's two row weights into the
 //     warp's row accumulators in shared memory. Lanes that write in the same
 //     instruction hold slices far enough apart that their rows differ, and the
@@ -37,13 +37,13 @@ namespace ctb {
 namespace {
 
 // a CTA: kFC detector columns (one warp each) x kFR * kRPL rows (kRPL per lane)
-constexpr int kFR = 32, kFC = 8, kRPL = 4;
+constexpr int kFR = 32, kFC = 8, kRPL = 8;
 constexpr unsigned kAll = 0xffffffffu;
 
 __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__ volz,
                                                        const float4* __restrict__ views, ProjGeom g,
                                                        float* __restrict__ proj, int accumulate) {
-    __shared__ float s_rows[kFC][kFR * kRPL];  // per warp: rows R .. R + 127
+    __shared__ float s_rows[kFC][kFR * kRPL];  // per warp: rows R .. R + 255
     const int lane = threadIdx.x;
     const int R = blockIdx.x * (kFR * kRPL);  // first row of the warp
     const int c = blockIdx.y * kFC + threadIdx.y;
@@ -125,8 +125,8 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                 const RowLine rl{__shfl_sync(kAll, mdv, j), __shfl_sync(kAll, c0, j)};
                 const float jinv = __shfl_sync(kAll, inv, j);
                 const int jcol = __shfl_sync(kAll, colidx, j);
-                // slices whose rows can reach R-1 .. R+127: box z in
-                // ((c0-R-129)/dv, (c0-R+1)/dv], dv = -mdv > 0, widened by m for the
+                // slices whose rows can reach R-1 .. R+255: box z in
+                // ((c0-R-257)/dv, (c0-R+1)/dv], dv = -mdv > 0, widened by m for the
                 // rounding of vi, of the quotients and of 1/dv (together below inv/16
                 // for rows under 2^17); the exact row test below decides
                 const float m = 0.08f * jinv + 0.01f;

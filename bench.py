@@ -174,7 +174,8 @@ def fp64_reference_slices(rows, cfg, geom, det, grid, z0, z1):
     V, _, W = rows.shape
     H = det.height
     vs = grid.voxel_pitch
-    g = orc.custom_geom(W, H, float(det.fcd), (grid.x_size, grid.y_size, grid.z_size), vs)
+    g = orc.custom_geom(W, H, float(det.fcd), (grid.x_size, grid.y_size, grid.z_size), vs,
+                        box=(grid.x_from, grid.x_to, grid.y_from, grid.y_to, grid.z_from, grid.z_to))
     ref = orc.f64_slices(rows, r0, H, geom.angles(), np.zeros(V), 1.0, FILTERS[cfg["filter"]], g, z0, z1)
     return ref  # (x, y, z1 - z0)
 
@@ -421,7 +422,10 @@ def run_ours(args):
     raw = scan.images
     angles = geom.angles()
     det, _ = ops.detector(W, H, geom.fcd_px)
-    grid = ops.custom_grid(det, (edge, edge, edge), vs)
+    # --subbox: the reference's xmin..zmax = 0.25..0.75 bounds (from/to = floor(f * size + 0.5))
+    rel = (0.25, 0.75) if args.subbox else (0.0, 1.0)
+    lo, hi = int(rel[0] * edge + 0.5), int(rel[1] * edge + 0.5)
+    grid = ops.custom_grid(det, (edge, edge, edge), vs, box=(lo, hi, lo, hi, lo, hi))
     X, Y, Z = grid.box
     units = float(X) * Y * Z * V
     slab = args.slab
@@ -505,6 +509,7 @@ def run_ours(args):
         v.setProjectionsPointer(host_in.data_ptr(), L.U16, V, W, H, angles, None, pixel_size=geom.pixel_eff,
                                 rotation="ccw", fcd_mm=geom.sod_mm, keep=host_in)
         v.setGrid(edge, edge, edge, vs)
+        v.setVolumeBounds(rel[0], rel[1], rel[0], rel[1], rel[0], rel[1])
         v.setFrequencyFilterType(cfg["filter"])
         v.setPrecision(args.store)
         v.setSlabHeight(slab)
@@ -561,9 +566,10 @@ def run_ours(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{args.config}: {V} views x {W}x{H} u16 -> {X}x{Y}x{Z} f32 (voxel {vs} px), "
-                               f"{cfg['filter']}, {args.store} storage", "storage": args.store,
+                               f"{cfg['filter']}, {args.store} storage"
+                               + (f", sub-box 0.25..0.75 of {edge}^3" if args.subbox else ""), "storage": args.store,
                    "views": V, "detector": [W, H], "volume": [X, Y, Z], "voxel_pitch_px": vs,
-                   "slab": slab, "l2": "inputs (12 GB) larger than L2; no flush", "parallelism": f"replicas{world}"},
+                   "slab": slab, "l2": f"inputs ({V * H * W * 2 / 1e9:.1f} GB raw) larger than L2 (126 MB); no flush", "parallelism": f"replicas{world}"},
         "recon_seconds": ms_per_step * 1e-3,
         "stage_ms": {"filter": main["filter_ms"], "backproject": main["bp_ms"]},
         "fp32": fp32,
@@ -648,6 +654,7 @@ def main():
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--store", default="fp16", choices=["fp16", "bf16", "fp32"])
     ap.add_argument("--slab", type=int, default=128)
+    ap.add_argument("--subbox", action="store_true", help="reconstruct the 0.25..0.75 sub-box in x, y and z")
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")

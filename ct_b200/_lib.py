@@ -112,6 +112,7 @@ SIGNATURES = {
     "ctb_batch_run_sequential": (I, [P, P]),
     "ctb_batch_tuning": (I, [P, P, P, P, P, P]),
     "ctb_device_wait_timeouts": (I, [I, P, I]),
+    "ctb_read_image": (I, [ctypes.c_char_p, P, P, P, P]),
     "ctb_diag_bounded_wait": (I, [I, ctypes.c_uint]),
     "ctb_batch_destroy": (None, [P]),
 }

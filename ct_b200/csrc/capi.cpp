@@ -10,6 +10,7 @@
 #include <string>
 
 #include "ctb_internal.h"
+#include "host/image_io.h"
 #include "host/reconstructor.h"
 
 struct ctb_ctx {
@@ -139,6 +140,20 @@ int ctb_backproject(const void* filtered, int store_type, int n_views, const dou
     st = ctb::backproject_launch(filtered, store_type, views, n_views, g, hmax, vol, accumulate, s);
     cudaFreeAsync(views, s);
     return st;
+}
+
+int ctb_read_image(const char* path, int* width, int* height, int* raw_type, void* out) {
+    if (!path || !width || !height || !raw_type) return arg_error("null pointer");
+    std::string err;
+    if (!ctb::probe_image(path, width, height, raw_type, &err)) {
+        ctb::set_global_error(err);
+        return CTB_ERR_IMAGE;
+    }
+    if (out && !ctb::decode_image_into(path, *width, *height, *raw_type, out, &err)) {
+        ctb::set_global_error(err);
+        return CTB_ERR_IMAGE;
+    }
+    return CTB_OK;
 }
 
 int ctb_device_wait_timeouts(int device, unsigned* count, int reset) {

@@ -164,11 +164,23 @@ bool tiff_info(const std::vector<uint8_t>& b, TiffInfo* t, std::string* err) {
         *err = "compressed TIFF is not supported (compression " + std::to_string(t->comp) + ")";
         return false;
     }
-    if (t->spp != 1) {
-        *err = "only single-channel TIFF is supported";
+    // colour (RGB, RGBA) is read as cv::imread(GRAYSCALE) does: converted to gray
+    const bool color = t->spp == 3 || t->spp == 4;
+    if (!(t->spp == 1 || (color && t->photo == 2 && t->planar == 1 && (t->bps == 8 || t->bps == 16)))) {
+        *err = "unsupported TIFF sample layout (" + std::to_string(t->spp) + " samples per pixel)";
         return false;
     }
     return true;
+}
+
+// cv::cvtColor RGB -> gray in 14-bit fixed point (R 4899, G 9617, B 1868), the
+// conversion cv::imread(IMREAD_GRAYSCALE) applies to colour TIFF images.
+template <typename T>
+void rgb_to_gray(const T* src, int channels, size_t n, T* dst) {
+    for (size_t i = 0; i < n; ++i) {
+        const T* p = src + i * channels;
+        dst[i] = T((uint32_t(p[0]) * 4899u + uint32_t(p[1]) * 9617u + uint32_t(p[2]) * 1868u + 8192u) >> 14);
+    }
 }
 
 int tiff_type(const TiffInfo& t) {
@@ -221,8 +233,9 @@ bool png_info(const std::vector<uint8_t>& b, PngInfo* p, bool want_data, std::st
         *err = "PNG without IHDR";
         return false;
     }
-    if (p->color != 0) {
-        *err = "only grayscale PNG is supported";
+    // gray (0), RGB (2), gray + alpha (4), RGBA (6); palettes are not read
+    if (p->color != 0 && p->color != 2 && p->color != 4 && p->color != 6) {
+        *err = "palette PNG is not supported";
         return false;
     }
     if (p->interlace != 0) {
@@ -236,8 +249,12 @@ bool png_info(const std::vector<uint8_t>& b, PngInfo* p, bool want_data, std::st
     return true;
 }
 
+int png_channels(int color) { return color == 2 ? 3 : color == 4 ? 2 : color == 6 ? 4 : 1; }
+
 bool png_decode(PngInfo& p, void* dst, std::string* err) {
-    const size_t bpp = p.depth / 8;
+    const int ch = png_channels(p.color);
+    const size_t bps = p.depth / 8;            // bytes per sample
+    const size_t bpp = bps * ch;               // bytes per pixel (filter unit)
     const size_t stride = size_t(p.w) * bpp;
     std::vector<uint8_t> raw((stride + 1) * size_t(p.h));
     uLongf out_len = uLongf(raw.size());
@@ -267,11 +284,17 @@ bool png_decode(PngInfo& p, void* dst, std::string* err) {
             }
             cur[c] = uint8_t(v);
         }
-        if (bpp == 1) {
-            std::memcpy(out + size_t(r) * stride, cur.data(), stride);
-        } else {
-            uint16_t* o = reinterpret_cast<uint16_t*>(out) + size_t(r) * p.w;
-            for (int c = 0; c < p.w; ++c) o[c] = uint16_t((cur[2 * c] << 8) | cur[2 * c + 1]);
+        // samples of this row (big-endian 16-bit), then one gray value per pixel:
+        // gray + alpha keeps the gray sample, colour goes through the gray formula
+        auto sample = [&](int c, int k) -> uint32_t {
+            const size_t o = size_t(c) * bpp + size_t(k) * bps;
+            return bps == 1 ? cur[o] : (uint32_t(cur[o]) << 8) | cur[o + 1];
+        };
+        for (int c = 0; c < p.w; ++c) {
+            uint32_t g = sample(c, 0);
+            if (ch >= 3) g = (sample(c, 0) * 4899u + sample(c, 1) * 9617u + sample(c, 2) * 1868u + 8192u) >> 14;
+            if (bps == 1) out[size_t(r) * p.w + c] = uint8_t(g);
+            else reinterpret_cast<uint16_t*>(out)[size_t(r) * p.w + c] = uint16_t(g);
         }
         std::swap(prev, cur);
     }
@@ -330,20 +353,25 @@ bool decode_image_into(const std::string& path, int width, int height, int type,
         if (!tiff_info(b, &t, err)) return false;
         const int ty = tiff_type(t);
         if (t.w != width || t.h != height || ty != type) { *err = "size or depth differs"; return false; }
-        const size_t sb = sample_bytes(ty), row = size_t(width) * sb;
+        const size_t sb = sample_bytes(ty), spp = size_t(t.spp), row = size_t(width) * sb * spp;
         const long rps = t.rows_per_strip > 0 ? t.rows_per_strip : height;
-        uint8_t* o = static_cast<uint8_t*>(dst);
+        std::vector<uint8_t> interleaved(spp > 1 ? n * sb * spp : 0);
+        uint8_t* o = spp > 1 ? interleaved.data() : static_cast<uint8_t*>(dst);
         size_t written = 0;
-        for (size_t s = 0; s < t.offsets.size() && written < n * sb; ++s) {
+        for (size_t s = 0; s < t.offsets.size() && written < n * sb * spp; ++s) {
             const size_t rows = std::min<size_t>(size_t(rps), size_t(height) - s * size_t(rps));
             const size_t bytes = rows * row;
             if (t.offsets[s] + bytes > b.size()) { *err = "truncated TIFF strip"; return false; }
             std::memcpy(o + written, b.data() + t.offsets[s], bytes);
             written += bytes;
         }
-        if (written != n * sb) { *err = "TIFF strips do not cover the image"; return false; }
+        if (written != n * sb * spp) { *err = "TIFF strips do not cover the image"; return false; }
         if (t.be && sb > 1) {
-            for (size_t i = 0; i < n; ++i) std::reverse(o + i * sb, o + (i + 1) * sb);
+            for (size_t i = 0; i < n * spp; ++i) std::reverse(o + i * sb, o + (i + 1) * sb);
+        }
+        if (spp > 1) {
+            if (sb == 1) rgb_to_gray(o, int(spp), n, static_cast<uint8_t*>(dst));
+            else rgb_to_gray(reinterpret_cast<const uint16_t*>(o), int(spp), n, static_cast<uint16_t*>(dst));
         }
         return true;
     }

@@ -219,6 +219,16 @@ def split_slices(weights, z: int) -> np.ndarray:
     return b
 
 
+def read_image(path: str) -> np.ndarray:
+    """One projection image decoded as the reference reads it (Projection::getImage)."""
+    w, h, t = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    check(lib().ctb_read_image(str(path).encode(), ctypes.byref(w), ctypes.byref(h), ctypes.byref(t), None))
+    dt = {L.U8: np.uint8, L.U16: np.uint16, L.F32: np.float32}[t.value]
+    out = np.empty((h.value, w.value), dt)
+    check(lib().ctb_read_image(str(path).encode(), ctypes.byref(w), ctypes.byref(h), ctypes.byref(t), out.ctypes.data))
+    return out
+
+
 def read_volume_info(txt_path: str) -> dict:
     """Dimensions and orders from a reconstruction's .txt info file (as the viewer reads it)."""
     x, y, z, io, bo = (ctypes.c_int() for _ in range(5))

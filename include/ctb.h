@@ -311,6 +311,17 @@ int ctb_device_wait_timeouts(int device, unsigned* count, int reset);
  * CTB_ERR_TIMEOUT (and adds 1 to the count) with the device still usable. */
 int ctb_diag_bounded_wait(int device, unsigned limit);
 
+/* ------------------------------------------------------ projection images */
+
+/* Projection::getImage (Ct/CtVolume.cpp:20-33): decode one projection image
+ * the way cv::imread(IMREAD_GRAYSCALE | IMREAD_ANYDEPTH) does for the formats
+ * read here: binary PGM (8/16-bit), uncompressed TIFF (8/16-bit integer,
+ * 32-bit float; gray, or RGB/RGBA converted to gray), PNG (8/16-bit gray,
+ * gray + alpha, RGB, RGBA). With out == NULL only the size and the sample
+ * type (CTB_U8 / CTB_U16 / CTB_F32) are returned; otherwise out receives
+ * width * height samples, row-major. */
+int ctb_read_image(const char* path, int* width, int* height, int* raw_type, void* out);
+
 /* ------------------------------------------------------ volume files */
 
 /* DataType, Common/types.h:27-36 (same order). */

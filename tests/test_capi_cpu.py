@@ -167,3 +167,43 @@ def test_missing_library_fails_loudly(monkeypatch):
     monkeypatch.setattr(L, "LIB_PATH", "/nonexistent/libctb.so")
     with pytest.raises(RuntimeError):
         L.lib()
+
+
+@pytest.mark.parametrize("depth", [np.uint8, np.uint16])
+def test_read_image_matches_cv2(tmp_path, depth):
+    """Projection images decoded as cv::imread(IMREAD_GRAYSCALE | IMREAD_ANYDEPTH) does: gray as is,
+    colour TIFF through cvtColor's 14-bit gray formula (bit-exact), colour PNG within the LSBs by which
+    libpng's own conversion differs from that formula, gray + alpha PNG without its alpha."""
+    cv2 = pytest.importorskip("cv2")
+    from ct_b200.ctvolume import read_image
+    rng = np.random.default_rng(int(np.iinfo(depth).max))
+    top = np.iinfo(depth).max
+    gray = rng.integers(0, top + 1, (23, 31)).astype(depth)
+    color = rng.integers(0, top + 1, (23, 31, 3)).astype(depth)      # BGR for cv2
+    rgba = rng.integers(0, top + 1, (23, 31, 4)).astype(depth)
+    flags = cv2.IMREAD_GRAYSCALE | cv2.IMREAD_ANYDEPTH
+    for name, img, ext, tol in [("g", gray, "png", 0), ("g", gray, "tif", 0), ("c", color, "tif", 0),
+                                ("a", rgba, "tif", 0), ("c", color, "png", 4), ("a", rgba, "png", 4)]:
+        path = str(tmp_path / f"{name}.{ext}")
+        params = [cv2.IMWRITE_TIFF_COMPRESSION, 1] if ext == "tif" else []   # uncompressed
+        assert cv2.imwrite(path, img, params)
+        ref = cv2.imread(path, flags)
+        got = read_image(path)
+        assert got.dtype == ref.dtype and got.shape == ref.shape, (name, ext)
+        diff = np.abs(got.astype(np.int64) - ref.astype(np.int64)).max()
+        assert diff <= tol, (name, ext, diff)
+    # gray + alpha PNG written by hand (cv2 writes no 2-channel PNG)
+    import struct
+    import zlib
+    ga = np.stack([gray, rng.integers(0, top + 1, gray.shape).astype(depth)], -1)
+    be = ">u2" if depth == np.uint16 else "u1"
+    raw = b"".join(b"\x00" + row.astype(be).tobytes() for row in ga)
+
+    def chunk(t, b):
+        return struct.pack(">I", len(b)) + t + b + struct.pack(">I", zlib.crc32(t + b) & 0xffffffff)
+    ihdr = struct.pack(">IIBBBBB", gray.shape[1], gray.shape[0], 8 * np.dtype(depth).itemsize, 4, 0, 0, 0)
+    path = str(tmp_path / "ga.png")
+    open(path, "wb").write(b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", ihdr) + chunk(b"IDAT", zlib.compress(raw)) +
+                           chunk(b"IEND", b""))
+    assert np.array_equal(read_image(path), cv2.imread(path, flags))
+    assert np.array_equal(read_image(path), gray)

@@ -91,7 +91,7 @@ bool pgm_header(const std::vector<uint8_t>& b, PgmHeader* hd, std::string* err) 
 
 // ----------------------------------------------------------------- TIFF
 struct TiffInfo {
-    int w = 0, h = 0, bps = 0, spp = 1, fmt = 1, comp = 1, photo = 1, planar = 1;
+    int w = 0, h = 0, bps = 0, spp = 1, fmt = 1, comp = 1, photo = 1, planar = 1, predictor = 1;
     long rows_per_strip = -1;
     std::vector<uint64_t> offsets, counts;
     bool be = false;
@@ -148,6 +148,7 @@ bool tiff_info(const std::vector<uint8_t>& b, TiffInfo* t, std::string* err) {
             case 278: t->rows_per_strip = long(value(0)); break;
             case 279: t->counts.resize(cnt); for (uint32_t i = 0; i < cnt; ++i) t->counts[i] = value(i); break;
             case 284: t->planar = int(value(0)); break;
+            case 317: t->predictor = int(value(0)); break;
             case 339: t->fmt = int(value(0)); break;
             default: break;
         }
@@ -160,8 +161,17 @@ bool tiff_info(const std::vector<uint8_t>& b, TiffInfo* t, std::string* err) {
         *err = "TIFF without size or strips";
         return false;
     }
-    if (t->comp != 1) {
-        *err = "compressed TIFF is not supported (compression " + std::to_string(t->comp) + ")";
+    // none, LZW, Deflate (two codes), PackBits; horizontal differencing for integers
+    if (t->comp != 1 && t->comp != 5 && t->comp != 8 && t->comp != 32946 && t->comp != 32773) {
+        *err = "unsupported TIFF compression " + std::to_string(t->comp);
+        return false;
+    }
+    if (t->predictor != 1 && !(t->predictor == 2 && t->fmt == 1)) {
+        *err = "unsupported TIFF predictor " + std::to_string(t->predictor);
+        return false;
+    }
+    if (t->counts.size() != t->offsets.size() && t->comp != 1) {
+        *err = "TIFF strip byte counts missing";
         return false;
     }
     // colour (RGB, RGBA) is read as cv::imread(GRAYSCALE) does: converted to gray
@@ -181,6 +191,76 @@ void rgb_to_gray(const T* src, int channels, size_t n, T* dst) {
         const T* p = src + i * channels;
         dst[i] = T((uint32_t(p[0]) * 4899u + uint32_t(p[1]) * 9617u + uint32_t(p[2]) * 1868u + 8192u) >> 14);
     }
+}
+
+// TIFF LZW (compression 5): MSB-first codes of 9..12 bits, clear 256, end 257,
+// the code width grows one code early (when the next free code reaches 2^n - 1).
+bool lzw_decode(const uint8_t* src, size_t n, uint8_t* dst, size_t cap, std::string* err) {
+    std::vector<uint16_t> prefix(4096), len(4096);
+    std::vector<uint8_t> suffix(4096), first(4096);
+    for (int i = 0; i < 256; ++i) { prefix[i] = 0xffff; suffix[i] = uint8_t(i); first[i] = uint8_t(i); len[i] = 1; }
+    size_t bitpos = 0, out = 0;
+    int width = 9, next = 258, prev = -1;
+    auto read = [&](int w) -> int {
+        if (bitpos + size_t(w) > n * 8) return 257;  // running out of data ends the strip
+        uint32_t v = 0;
+        for (int k = 0; k < w; ++k, ++bitpos) v = (v << 1) | ((src[bitpos >> 3] >> (7 - (bitpos & 7))) & 1u);
+        return int(v);
+    };
+    auto emit = [&](int code) -> bool {
+        const size_t l = len[code];
+        if (out + l > cap) return false;
+        size_t at = out + l;
+        for (int c = code; c != 0xffff; c = prefix[c]) dst[--at] = suffix[c];
+        out += l;
+        return true;
+    };
+    while (out < cap) {
+        const int code = read(width);
+        if (code == 257) break;
+        if (code == 256) { width = 9; next = 258; prev = -1; continue; }
+        if (prev < 0) {
+            if (code > 255) { *err = "corrupt LZW data"; return false; }
+            if (!emit(code)) break;
+            prev = code;
+            continue;
+        }
+        if (code > next || next >= 4096) { *err = "corrupt LZW data"; return false; }
+        // new entry: string(prev) + first byte of string(code), or of string(prev) when code is new
+        const uint8_t f = code < next ? first[code] : first[prev];
+        prefix[next] = uint16_t(prev);
+        suffix[next] = f;
+        first[next] = first[prev];
+        len[next] = uint16_t(len[prev] + 1);
+        ++next;
+        if (!emit(code)) break;
+        prev = code;
+        if (next + 1 >= (1 << width) && width < 12) ++width;
+    }
+    if (out != cap) { *err = "LZW strip shorter than its rows"; return false; }
+    return true;
+}
+
+// PackBits (compression 32773).
+bool packbits_decode(const uint8_t* src, size_t n, uint8_t* dst, size_t cap, std::string* err) {
+    size_t i = 0, out = 0;
+    while (i < n && out < cap) {
+        const int8_t h = int8_t(src[i++]);
+        if (h >= 0) {
+            const size_t k = size_t(h) + 1;
+            if (i + k > n || out + k > cap) break;
+            std::memcpy(dst + out, src + i, k);
+            i += k;
+            out += k;
+        } else if (h != -128) {
+            const size_t k = size_t(1 - h);
+            if (i >= n || out + k > cap) break;
+            std::memset(dst + out, src[i++], k);
+            out += k;
+        }
+    }
+    if (out != cap) { *err = "PackBits strip shorter than its rows"; return false; }
+    return true;
 }
 
 int tiff_type(const TiffInfo& t) {
@@ -361,13 +441,42 @@ bool decode_image_into(const std::string& path, int width, int height, int type,
         for (size_t s = 0; s < t.offsets.size() && written < n * sb * spp; ++s) {
             const size_t rows = std::min<size_t>(size_t(rps), size_t(height) - s * size_t(rps));
             const size_t bytes = rows * row;
-            if (t.offsets[s] + bytes > b.size()) { *err = "truncated TIFF strip"; return false; }
-            std::memcpy(o + written, b.data() + t.offsets[s], bytes);
+            if (t.comp == 1) {
+                if (t.offsets[s] + bytes > b.size()) { *err = "truncated TIFF strip"; return false; }
+                std::memcpy(o + written, b.data() + t.offsets[s], bytes);
+            } else {
+                if (t.offsets[s] + t.counts[s] > b.size()) { *err = "truncated TIFF strip"; return false; }
+                const uint8_t* src = b.data() + t.offsets[s];
+                const size_t cn = size_t(t.counts[s]);
+                if (t.comp == 5) {
+                    if (!lzw_decode(src, cn, o + written, bytes, err)) return false;
+                } else if (t.comp == 32773) {
+                    if (!packbits_decode(src, cn, o + written, bytes, err)) return false;
+                } else {  // Deflate: a zlib stream per strip
+                    uLongf got = uLongf(bytes);
+                    if (uncompress(o + written, &got, src, uLong(cn)) != Z_OK || got != bytes) {
+                        *err = "TIFF Deflate strip failed to inflate";
+                        return false;
+                    }
+                }
+            }
             written += bytes;
         }
         if (written != n * sb * spp) { *err = "TIFF strips do not cover the image"; return false; }
         if (t.be && sb > 1) {
             for (size_t i = 0; i < n * spp; ++i) std::reverse(o + i * sb, o + (i + 1) * sb);
+        }
+        if (t.predictor == 2) {  // horizontal differencing, per sample channel, within each row
+            const size_t rs = size_t(width) * spp;
+            for (int r = 0; r < height; ++r) {
+                if (sb == 1) {
+                    uint8_t* v = o + size_t(r) * rs;
+                    for (size_t i = spp; i < rs; ++i) v[i] = uint8_t(v[i] + v[i - spp]);
+                } else {
+                    uint16_t* v = reinterpret_cast<uint16_t*>(o) + size_t(r) * rs;
+                    for (size_t i = spp; i < rs; ++i) v[i] = uint16_t(v[i] + v[i - spp]);
+                }
+            }
         }
         if (spp > 1) {
             if (sb == 1) rgb_to_gray(o, int(spp), n, static_cast<uint8_t*>(dst));

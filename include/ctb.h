@@ -315,8 +315,9 @@ int ctb_diag_bounded_wait(int device, unsigned limit);
 
 /* Projection::getImage (Ct/CtVolume.cpp:20-33): decode one projection image
  * the way cv::imread(IMREAD_GRAYSCALE | IMREAD_ANYDEPTH) does for the formats
- * read here: binary PGM (8/16-bit), uncompressed TIFF (8/16-bit integer,
- * 32-bit float; gray, or RGB/RGBA converted to gray), PNG (8/16-bit gray,
+ * read here: binary PGM (8/16-bit), TIFF strips (8/16-bit integer, 32-bit
+ * float; uncompressed, LZW, Deflate or PackBits, with or without horizontal
+ * differencing; gray, or RGB/RGBA converted to gray), PNG (8/16-bit gray,
  * gray + alpha, RGB, RGBA). With out == NULL only the size and the sample
  * type (CTB_U8 / CTB_U16 / CTB_F32) are returned; otherwise out receives
  * width * height samples, row-major. */

@@ -207,3 +207,25 @@ def test_read_image_matches_cv2(tmp_path, depth):
                            chunk(b"IEND", b""))
     assert np.array_equal(read_image(path), cv2.imread(path, flags))
     assert np.array_equal(read_image(path), gray)
+
+
+@pytest.mark.parametrize("depth", [np.uint8, np.uint16])
+@pytest.mark.parametrize("compression", [1, 5, 8, 32946, 32773])
+def test_read_compressed_tiff_matches_cv2(tmp_path, depth, compression):
+    """TIFF strips without compression, LZW, Deflate and PackBits, with the horizontal predictor OpenCV
+    writes by default, gray and colour: identical to cv2.imread(IMREAD_GRAYSCALE | IMREAD_ANYDEPTH)."""
+    cv2 = pytest.importorskip("cv2")
+    from ct_b200.ctvolume import read_image
+    rng = np.random.default_rng(compression)
+    top = np.iinfo(depth).max
+    yy, xx = np.mgrid[0:181, 0:263]
+    smooth = (np.sin(xx / 17.0) * np.cos(yy / 11.0) * 0.5 + 0.5) * top * 0.8
+    gray = np.clip(smooth + rng.normal(0, top * 0.02, smooth.shape), 0, top).astype(depth)
+    color = np.stack([gray, np.roll(gray, 5, 1), rng.integers(0, top + 1, gray.shape).astype(depth)], -1)
+    flags = cv2.IMREAD_GRAYSCALE | cv2.IMREAD_ANYDEPTH
+    for name, img in [("g", gray), ("c", color)]:
+        path = str(tmp_path / f"{name}{compression}.tif")
+        assert cv2.imwrite(path, img, [cv2.IMWRITE_TIFF_COMPRESSION, compression])
+        ref = cv2.imread(path, flags)
+        got = read_image(path)
+        assert got.dtype == ref.dtype and np.array_equal(got, ref), (name, compression)

@@ -46,6 +46,14 @@ class Scan(ctypes.Structure):
                 ("grid", Grid), ("filter", ctypes.c_int32), ("pad", ctypes.c_int32), ("vol", ctypes.c_void_p)]
 
 
+class Settings(ctypes.Structure):
+    _fields_ = [("skip_projections", ctypes.c_uint), ("use_cuda", ctypes.c_int),
+                ("use_cpu_preprocessing", ctypes.c_int), ("emit_signals", ctypes.c_int),
+                ("gpu_spare_memory_mb", ctypes.c_size_t), ("multiprocessor_coefficient", ctypes.c_double),
+                ("memory_bandwidth_coefficient", ctypes.c_double), ("n_devices", ctypes.c_int),
+                ("devices", ctypes.c_int * 16)]
+
+
 class Timings(ctypes.Structure):
     _fields_ = [("upload_s", ctypes.c_double), ("filter_s", ctypes.c_double), ("backproject_s", ctypes.c_double),
                 ("download_s", ctypes.c_double), ("total_s", ctypes.c_double), ("voxel_views", ctypes.c_double)]
@@ -113,6 +121,12 @@ SIGNATURES = {
     "ctb_batch_tuning": (I, [P, P, P, P, P, P]),
     "ctb_device_wait_timeouts": (I, [I, P, I]),
     "ctb_read_image": (I, [ctypes.c_char_p, P, P, P, P]),
+    "ctb_set_use_cuda": (I, [P, I]),
+    "ctb_set_use_cpu_preprocessing": (I, [P, I]),
+    "ctb_set_emit_signals": (I, [P, I]),
+    "ctb_get_settings": (I, [P, P]),
+    "ctb_get_required_memory": (I, [P, P]),
+    "ctb_get_projection": (I, [P, I, P, P, P]),
     "ctb_diag_bounded_wait": (I, [I, ctypes.c_uint]),
     "ctb_batch_destroy": (None, [P]),
 }

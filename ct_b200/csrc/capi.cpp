@@ -367,6 +367,34 @@ void ctb_stop(ctb_ctx* ctx) {
     if (ctx) ctx->r.stop();
 }
 
+int ctb_set_use_cuda(ctb_ctx* ctx, int v) { CTX_CHECK(ctx); return ctx->r.set_use_cuda(v != 0); }
+int ctb_set_use_cpu_preprocessing(ctb_ctx* ctx, int v) {
+    CTX_CHECK(ctx);
+    ctx->r.set_use_cpu_preprocessing(v != 0);
+    return CTB_OK;
+}
+int ctb_set_emit_signals(ctb_ctx* ctx, int v) {
+    CTX_CHECK(ctx);
+    ctx->r.set_emit_signals(v != 0);
+    return CTB_OK;
+}
+int ctb_get_settings(const ctb_ctx* ctx, ctb_settings* s) {
+    CTX_CHECK(ctx);
+    if (!s) return arg_error("null pointer");
+    ctx->r.settings(s);
+    return CTB_OK;
+}
+int ctb_get_required_memory(const ctb_ctx* ctx, size_t* bytes) {
+    CTX_CHECK(ctx);
+    if (!bytes) return arg_error("null pointer");
+    *bytes = ctx->r.required_memory();
+    return CTB_OK;
+}
+int ctb_get_projection(ctb_ctx* ctx, int index, float* image, double* angle_deg, double* height_offset_px) {
+    CTX_CHECK(ctx);
+    return ctx->r.projection(index, image, angle_deg, height_offset_px);
+}
+
 int ctb_get_timings(const ctb_ctx* ctx, ctb_timings* t) {
     CTX_CHECK(ctx);
     if (!t) return arg_error("null pointer");

@@ -267,6 +267,82 @@ int Reconstructor::set_filter(int f) {
     return CTB_OK;
 }
 
+// setUseCuda (:502-504): the reconstruction runs on the GPU only.
+int Reconstructor::set_use_cuda(bool v) {
+    if (!v) return fail(CTB_ERR_UNSUPPORTED, "CPU reconstruction is not part of this engine; it reconstructs on the GPU.");
+    return CTB_OK;
+}
+
+void Reconstructor::settings(ctb_settings* s) const {
+    *s = ctb_settings{};
+    s->skip_projections = unsigned(std::max(1, step_) - 1);  // getSkipProjections (:438-440)
+    s->use_cuda = 1;
+    s->use_cpu_preprocessing = cpu_pre_ ? 1 : 0;
+    s->emit_signals = emit_ ? 1 : 0;
+    s->gpu_spare_memory_mb = spare_mb_;
+    s->multiprocessor_coefficient = mp_coef_;
+    s->memory_bandwidth_coefficient = bw_coef_;
+    s->n_devices = int(std::min<size_t>(devices_.size(), 16));
+    for (int i = 0; i < s->n_devices; ++i) s->devices[i] = devices_[i];
+}
+
+// getRequiredMemoryUpperBound (:469-481), CUDA branch: the float volume plus
+// three float images per active device.
+size_t Reconstructor::required_memory() const {
+    const size_t X = size_t(std::max(0, grid_.x_to - grid_.x_from));
+    const size_t Y = size_t(std::max(0, grid_.y_to - grid_.y_from));
+    const size_t Z = size_t(std::max(0, grid_.z_to - grid_.z_from));
+    return X * Y * Z * sizeof(float) +
+           size_t(det_.width) * size_t(det_.height) * sizeof(float) * devices_.size() * 3;
+}
+
+// getProjectionAt (:332-341): the image converted to float as convertTo32bit
+// does (:802-812) and normalised by the scan's minimum and maximum, which the
+// reference gathers while loading (:270-292): raw extremes divided by 2^8 for
+// 8-bit images and by 2^16 otherwise.
+int Reconstructor::projection(int index, float* image, double* angle_deg, double* height_px) {
+    if (!have_scan_ || index < 0 || index >= int(angles_.size())) return fail(CTB_ERR_ARG, "Index out of bounds.");
+    if (angle_deg) *angle_deg = angles_[index];
+    if (height_px) *height_px = heights_px_[index];
+    if (!image) return CTB_OK;
+    const size_t n = size_t(det_.width) * det_.height;
+    auto sample = [&](size_t v, size_t i) -> double {
+        if (raw_type_ == CTB_U8) return static_cast<const uint8_t*>(images_)[v * n + i];
+        if (raw_type_ == CTB_U16) return static_cast<const uint16_t*>(images_)[v * n + i];
+        return static_cast<const float*>(images_)[v * n + i];
+    };
+    if (!have_minmax_) {
+        const size_t V = angles_.size();
+        std::vector<double> lo(V), hi(V);
+        parallel_for(V, [&](size_t v) {
+            double a = sample(v, 0), b = a;
+            for (size_t i = 1; i < n; ++i) {
+                const double x = sample(v, i);
+                a = std::min(a, x);
+                b = std::max(b, x);
+            }
+            lo[v] = a;
+            hi[v] = b;
+        });
+        const double scale = raw_type_ == CTB_U8 ? 256.0 : 65536.0;
+        min_max_[0] = float(*std::min_element(lo.begin(), lo.end()) / scale);
+        min_max_[1] = float(*std::max_element(hi.begin(), hi.end()) / scale);
+        have_minmax_ = true;
+    }
+    const float alpha = float(raw_type_ == CTB_U8 ? 1.0 / 255.0 : 1.0 / 65535.0);
+    const float beta = float(0.000001 * double(det_.base_intensity));
+    const float lo = min_max_[0], span = min_max_[1] - min_max_[0];
+    for (size_t i = 0; i < n; ++i) {
+        float p = float(sample(size_t(index), i));
+        if (raw_type_ != CTB_F32) {
+            const float scaled = p * alpha;  // separate statements: no fused multiply-add
+            p = scaled + beta;
+        }
+        image[i] = (p - lo) / span;
+    }
+    return CTB_OK;
+}
+
 int Reconstructor::set_device(int d) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || d < 0 || d >= n) {
@@ -502,6 +578,7 @@ int Reconstructor::assign_scan(const void* images, int raw_type, int n_views, in
             for (double& v : angles_) v *= -1;
     }
     have_scan_ = true;
+    have_minmax_ = false;
     update_grid();
     cs_index_ = std::max(0, box_extent(cs_axis_)) / 2;  // (:317-326)
     return CTB_OK;
@@ -523,7 +600,7 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
                         "The memory allocation for the volume failed. Maybe there is not enought free RAM.");
         target = static_cast<float*>(volume_.p);
         index_order = CTB_X_FASTEST;
-        if (preview_) {  // previews show the unfinished part as zeros (reinitialise, :555)
+        if (previews()) {  // previews show the unfinished part as zeros (reinitialise, :555)
             const size_t n = size_t(X) * Y * Z, parts = 16;
             parallel_for(parts, [&](size_t p) {
                 std::memset(target + p * n / parts, 0, sizeof(float) * ((p + 1) * n / parts - p * n / parts));
@@ -574,7 +651,7 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
     }
     if (!host_out) {
         vol_dims_[0] = X; vol_dims_[1] = Y; vol_dims_[2] = Z;
-        if (preview_) emit_preview(target, 100.0);  // reconstructionFinished (:615)
+        if (previews()) emit_preview(target, 100.0);  // reconstructionFinished (:615)
     }
 
     ctb_timings t{};
@@ -599,7 +676,7 @@ void Reconstructor::worker_progress(DeviceWork& w, double frac, const float* pre
     double total = 0;
     for (auto& o : workers_) total += o->progress * o->share;
     progress(1, 100.0 * total);
-    if (preview_ && preview_vol) emit_preview(preview_vol, 100.0 * total);
+    if (previews() && preview_vol) emit_preview(preview_vol, 100.0 * total);
 }
 
 // Reconstructs box slices [z_lo, z_hi) on worker w's device into out, which
@@ -846,7 +923,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         cudaEventRecord(ev_down[b], w.s_down);
         // previews read the context's own volume up to the previous slab, which
         // has landed by now (waiting for this one would stall the next launch)
-        const bool preview = preview_ && out == static_cast<float*>(volume_.p) && out_pinned && k >= 1;
+        const bool preview = previews() && out == static_cast<float*>(volume_.p) && out_pinned && k >= 1;
         if (preview) cudaEventSynchronize(ev_down[(k - 1) % 2]);
         worker_progress(w, double(k + 1) / double(nslabs), preview ? out : nullptr);
     }

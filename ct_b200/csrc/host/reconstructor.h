@@ -95,6 +95,10 @@ class Reconstructor {
     int cross_section_axis() const { return cs_axis_; }
     int cross_section_index() const { return cs_index_; }
     int cross_section_size() const;
+    // setEmitSignals / setUseCuda / setUseCpuPreprocessing (Ct/CtVolume.h:99-110)
+    void set_emit_signals(bool v) { emit_ = v; }
+    int set_use_cuda(bool v);
+    void set_use_cpu_preprocessing(bool v) { cpu_pre_ = v; }
 
     // ---- getters
     const ctb_detector& detector() const { return det_; }
@@ -102,6 +106,11 @@ class Reconstructor {
     int views() const { return int(angles_.size()); }
     double pixel_size() const { return pixel_size_; }
     const ctb_timings& timings() const { return tm_; }
+    void settings(ctb_settings* s) const;
+    size_t required_memory() const;
+    // getProjectionAt: angle, relative height offset (pixels) and, if image is
+    // given, the raw image as float normalised by the scan's min / max
+    int projection(int index, float* image, double* angle_deg, double* height_px);
 
     // ---- work
     int reconstruct(float* host_out, int index_order);   // host_out == nullptr: keep internally
@@ -119,7 +128,8 @@ class Reconstructor {
                     double u_offset_mm, double fcd_mm, double base_intensity);
     void update_grid();
     int run_pipeline(DeviceWork& w, float* host_out, int index_order, int z_lo, int z_hi);
-    void progress(int stage, double pct) { if (cb_) cb_(stage, pct, cb_user_); }
+    void progress(int stage, double pct) { if (cb_ && emit_) cb_(stage, pct, cb_user_); }
+    bool previews() const { return preview_ && emit_; }
     void worker_progress(DeviceWork& w, double frac, const float* preview_vol = nullptr);
     void emit_preview(const float* vol, double pct);
     int box_extent(int axis) const;
@@ -157,6 +167,10 @@ class Reconstructor {
     std::vector<float> preview_buf_;
     int cs_axis_ = CTB_AXIS_Z;       // crossSectionAxis (:239)
     int cs_index_ = 0;               // crossSectionIndex (:238)
+    bool emit_ = true;               // emitSignals: progress / preview callbacks
+    bool cpu_pre_ = false;           // useCpuPreprocessing (accepted, no effect)
+    bool have_minmax_ = false;       // minMaxValues (:292), computed on first use
+    float min_max_[2] = {0, 0};
 
     // geometry (updateBoundaries)
     ctb_grid grid_{};

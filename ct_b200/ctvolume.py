@@ -169,6 +169,63 @@ class CtVolume:
         self._ck(lib().ctb_get_cross_section(self._ctx, axis, index, out.ctypes.data, None, None))
         return out
 
+    # ------------------------------------------------ remaining CtVolume getters / setters
+    @staticmethod
+    def getCudaDeviceCount() -> int:
+        n = ctypes.c_int()
+        return n.value if lib().ctb_device_count(ctypes.byref(n)) == L.CTB_OK else -1
+
+    @staticmethod
+    def cudaAvailable() -> bool:
+        return CtVolume.getCudaDeviceCount() > 0
+
+    def getCudaDeviceList(self):
+        names = []
+        for i in range(max(0, self.getCudaDeviceCount())):
+            buf = ctypes.create_string_buffer(256)
+            lib().ctb_device_name(i, buf, 256)
+            names.append(buf.value.decode(errors="replace"))
+        return names
+
+    def _settings(self) -> L.Settings:
+        s = L.Settings()
+        self._ck(lib().ctb_get_settings(self._ctx, ctypes.byref(s)))
+        return s
+
+    def getSkipProjections(self): return self._settings().skip_projections
+    def getUseCuda(self): return bool(self._settings().use_cuda)
+    def getUseCpuPreprocessing(self): return bool(self._settings().use_cpu_preprocessing)
+    def getEmitSignals(self): return bool(self._settings().emit_signals)
+    def getGpuSpareMemory(self): return self._settings().gpu_spare_memory_mb
+    def getMultiprocessorCoefficient(self): return self._settings().multiprocessor_coefficient
+    def getMemoryBandwidthCoefficient(self): return self._settings().memory_bandwidth_coefficient
+
+    def getActiveCudaDevices(self):
+        s = self._settings()
+        return [s.devices[i] for i in range(s.n_devices)]
+
+    def getRequiredMemoryUpperBound(self) -> int:
+        n = ctypes.c_size_t()
+        self._ck(lib().ctb_get_required_memory(self._ctx, ctypes.byref(n)))
+        return n.value
+
+    def setUseCuda(self, value: bool):
+        self._ck(lib().ctb_set_use_cuda(self._ctx, int(bool(value))))
+
+    def setUseCpuPreprocessing(self, value: bool):
+        self._ck(lib().ctb_set_use_cpu_preprocessing(self._ctx, int(bool(value))))
+
+    def setEmitSignals(self, value: bool):
+        self._ck(lib().ctb_set_emit_signals(self._ctx, int(bool(value))))
+
+    def getProjectionAt(self, index: int):
+        """(image normalised by the scan's min / max as float32 (H, W), angle in degrees, height offset in pixels)."""
+        w, h = self.getImageWidth(), self.getImageHeight()
+        img = np.empty((h, w), np.float32)
+        a, o = ctypes.c_double(), ctypes.c_double()
+        self._ck(lib().ctb_get_projection(self._ctx, int(index), img.ctypes.data, ctypes.byref(a), ctypes.byref(o)))
+        return img, a.value, o.value
+
     def setCrossSectionAxis(self, axis: int):
         self._ck(lib().ctb_set_cross_section_axis(self._ctx, int(axis)))
 

@@ -260,6 +260,15 @@ int ctb_set_grid(ctb_ctx* ctx, int x_size, int y_size, int z_size, float voxel_p
 int ctb_set_slab_height(ctb_ctx* ctx, int slices);        /* 0 = automatic */
 int ctb_set_progress_callback(ctb_ctx* ctx, ctb_progress_cb cb, void* user);
 
+/* setUseCuda (Ct/CtVolume.h:104): 0 is refused (CTB_ERR_UNSUPPORTED), the
+ * engine reconstructs on the GPU only. setUseCpuPreprocessing (:111) is
+ * accepted and has no effect: preprocessing always runs on the GPU.
+ * setEmitSignals (:100): 0 silences the progress and preview callbacks, as
+ * the reference silences its Qt signals. */
+int ctb_set_use_cuda(ctb_ctx* ctx, int use_cuda);
+int ctb_set_use_cpu_preprocessing(ctb_ctx* ctx, int value);
+int ctb_set_emit_signals(ctb_ctx* ctx, int value);
+
 /* Getters (Ct/CtVolume.h:69-94). */
 int ctb_get_detector(const ctb_ctx* ctx, ctb_detector* det);
 int ctb_get_grid(const ctb_ctx* ctx, ctb_grid* grid);
@@ -296,6 +305,33 @@ typedef struct {
     double voxel_views;     /* x*y*z*views processed */
 } ctb_timings;
 int ctb_get_timings(const ctb_ctx* ctx, ctb_timings* t);
+
+/* getSkipProjections, getUseCuda, getUseCpuPreprocessing, getEmitSignals,
+ * getGpuSpareMemory, getMultiprocessorCoefficient,
+ * getMemoryBandwidthCoefficient, getActiveCudaDevices (Ct/CtVolume.h:86-95). */
+typedef struct {
+    unsigned skip_projections;
+    int use_cuda;                 /* always 1 */
+    int use_cpu_preprocessing;
+    int emit_signals;
+    size_t gpu_spare_memory_mb;
+    double multiprocessor_coefficient;
+    double memory_bandwidth_coefficient;
+    int n_devices;                /* active devices (the first 16 listed) */
+    int devices[16];
+} ctb_settings;
+int ctb_get_settings(const ctb_ctx* ctx, ctb_settings* s);
+/* getRequiredMemoryUpperBound (Ct/CtVolume.cpp:469-481): bytes of host memory
+ * the reference would need: the float volume plus three float images per
+ * active device. */
+int ctb_get_required_memory(const ctb_ctx* ctx, size_t* bytes);
+/* getProjectionAt (Ct/CtVolume.cpp:332-341): the view's angle (degrees,
+ * direction-corrected), its relative height offset (pixels) and, if image is
+ * not NULL, width*height floats: the raw image scaled as the reference's
+ * convertTo32bit and normalised by the scan's minimum and maximum sample
+ * (divided by 2^8 for 8-bit scans, 2^16 otherwise, as the reference does).
+ * CTB_ERR_ARG for an index out of bounds. */
+int ctb_get_projection(ctb_ctx* ctx, int index, float* image, double* angle_deg, double* height_offset_px);
 
 /* --------------------------------------------------- device waits */
 

@@ -229,3 +229,40 @@ def test_read_compressed_tiff_matches_cv2(tmp_path, depth, compression):
         ref = cv2.imread(path, flags)
         got = read_image(path)
         assert got.dtype == ref.dtype and np.array_equal(got, ref), (name, compression)
+
+
+def test_remaining_facade_getters_and_setters(tmp_path):
+    """getProjectionAt, getSkipProjections, getUseCuda, getEmitSignals, getActiveCudaDevices,
+    getGpuSpareMemory, the GPU coefficients and getRequiredMemoryUpperBound (Ct/CtVolume.cpp:332-481)."""
+    csv, imgs, geom = write_scan(tmp_path, heights=[0.0, 0.5, 1.0, 1.5, 2.0, 2.5])
+    v = CtVolume(csv)
+    # getProjectionAt: convertTo32bit then (p - min) / (max - min) with min, max = raw extremes / 2^16
+    img, angle, height = v.getProjectionAt(2)
+    lo, hi = np.float32(imgs.min() / 65536.0), np.float32(imgs.max() / 65536.0)
+    alpha, beta = np.float32(1.0 / 65535.0), np.float32(0.000001 * 1.0)
+    p = imgs[2].astype(np.float32) * alpha + beta
+    np.testing.assert_array_equal(img, (p - lo) / (hi - lo))
+    assert angle == pytest.approx(geom.angles()[2])
+    pix = v.getPixelSize()
+    assert height == pytest.approx((1.0 - 1.25) / pix)        # relative to the mean, in pixels
+    with pytest.raises(CtbError):
+        v.getProjectionAt(6)
+    # settings
+    assert v.getSkipProjections() == 0 and v.getUseCuda() and v.getEmitSignals()
+    assert not v.getUseCpuPreprocessing() and v.getGpuSpareMemory() == 200
+    assert (v.getMultiprocessorCoefficient(), v.getMemoryBandwidthCoefficient()) == (1.0, 1.0)
+    assert v.getActiveCudaDevices() == [0]
+    v.setSkipProjections(3)
+    v.setGpuSpareMemory(512)
+    v.setGpuCoefficients(2.0, 0.5)
+    v.setUseCpuPreprocessing(True)
+    v.setEmitSignals(False)
+    assert v.getSkipProjections() == 3 and v.getGpuSpareMemory() == 512
+    assert (v.getMultiprocessorCoefficient(), v.getMemoryBandwidthCoefficient()) == (2.0, 0.5)
+    assert v.getUseCpuPreprocessing() and not v.getEmitSignals()
+    with pytest.raises(CtbError):
+        v.setUseCuda(False)
+    v.setUseCuda(True)
+    X, Y, Z = v.getXSize(), v.getYSize(), v.getZSize()
+    assert v.getRequiredMemoryUpperBound() == X * Y * Z * 4 + 12 * 8 * 4 * 1 * 3
+    assert isinstance(CtVolume.cudaAvailable(), bool)

@@ -386,3 +386,17 @@ def test_forward_is_the_exact_transpose(vs, uoff, heights):
     assert np.count_nonzero(A) > 100
     assert np.array_equal(A != 0, At.T != 0)
     np.testing.assert_allclose(A, At.T, rtol=1e-6, atol=1e-7)
+
+
+def test_emit_signals_off_silences_callbacks(tmp_path):
+    csv, imgs, geom = c1_scan(tmp_path, n_views=20, W=48, H=32)
+    v = CtVolume(csv)
+    seen = []
+    v.setProgressCallback(lambda s, p: seen.append(p))
+    v.setPreviewCallback(lambda p, sec: seen.append(p))
+    v.setEmitSignals(False)
+    v.reconstructVolume()
+    assert seen == []
+    v.setEmitSignals(True)
+    v.reconstructVolume()
+    assert seen and seen[-1] == 100.0

@@ -91,7 +91,8 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ pro
 #pragma unroll
             for (int j = 0; j < ZC; ++j) {
                 const float vi = row_at(rl, float(g.z_begin + z0 + j));
-                if (row_ok(vi, g.vi_hi)) {
+                const float zw = __fmul_rn(__fsub_rn(float(z0 + j), g.zPre), g.vs);
+                if (v_inside(zw, q.z, U, g.lbV, g.ubV)) {
                     const int v0 = int(vi);
                     const float fv = __fsub_rn(vi, float(v0));
                     const T* r0 = col + (long long)v0 * g.pitch;

@@ -266,7 +266,8 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                     const T* col = buf + size_t(b) * buf_stride + (u0 - o.x) - o.y * bx.BU;
                     const int BU = bx.BU;
                     // strictly inside the row bounds (half-pixel margin): every voxel of the column passes
-                    // the per-voxel test, so this loop and the checked one take the same decisions
+                    // the per-voxel membership test, so this loop and the checked one take the same
+                    // decisions
                     if (fminf(vf, vl) >= 0.5f && fmaxf(vf, vl) <= g.vi_hi - 0.5f) {
 #pragma unroll
                         for (int j = 0; j < ZC; ++j) {
@@ -281,10 +282,12 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                             acc[j] = fmaf(w, fmaf(fv, c - a, a), acc[j]);
                         }
                     } else {
+                        int ja, jb;
+                        v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);
 #pragma unroll
                         for (int j = 0; j < ZC; ++j) {
                             const float vi = row_at(rl, zf[j]);
-                            if (row_ok(vi, g.vi_hi)) {
+                            if (j >= ja && j <= jb) {
                                 const int v0 = int(vi);
                                 const float fv = __fsub_rn(vi, float(v0));
                                 const T* r0 = col + v0 * BU;
@@ -298,10 +301,12 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                     }
                 } else {
                     const T* col = proj + (long long)iv * g.view_stride + u0;
+                    int ja, jb;
+                    v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);
 #pragma unroll
                     for (int j = 0; j < ZC; ++j) {
                         const float vi = row_at(rl, zf[j]);
-                        if (row_ok(vi, g.vi_hi)) {
+                        if (j >= ja && j <= jb) {
                             const int v0 = int(vi);
                             const float fv = __fsub_rn(vi, float(v0));
                             const T* r0 = col + (long long)v0 * g.pitch;

@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
         for (int st = 0; st < steps; ++st) {
             // (2) this lane's candidate column for this step
             bool hit = false;
-            float wb = 0.0f, mdv = 0.0f, c0 = 0.0f, inv = 0.0f;
+            float wb = 0.0f, mdv = 0.0f, c0 = 0.0f, inv = 0.0f, Uc = 0.0f;
             int colidx = 0;
             if (st < cnt) {
                 const int is = i0 + st;
@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                             mdv = rl.mdv;
                             c0 = rl.c0;
                             inv = 1.0f / -rl.mdv;
+                            Uc = U;
                             colidx = x * g.Y + y;
                         }
                     }
@@ -125,6 +126,7 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                 const RowLine rl{__shfl_sync(kAll, mdv, j), __shfl_sync(kAll, c0, j)};
                 const float jinv = __shfl_sync(kAll, inv, j);
                 const int jcol = __shfl_sync(kAll, colidx, j);
+                const float jU = __shfl_sync(kAll, Uc, j);
                 // slices whose rows can reach R-1 .. R+255: box z in
                 // ((c0-R-257)/dv, (c0-R+1)/dv], dv = -mdv > 0, widened by m for the
                 // rounding of vi, of the quotients and of 1/dv (together below inv/16
@@ -148,7 +150,8 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                         float ca = 0.0f, cb = 0.0f;
                         if (z <= z1) {
                             const float vi = row_at(rl, float(g.z_begin + z));
-                            if (row_ok(vi, g.vi_hi)) {
+                            const float zw = __fmul_rn(__fsub_rn(float(z), g.zPre), g.vs);
+                            if (v_inside(zw, h, jU, g.lbV, g.ubV)) {
                                 const int v0 = int(vi);
                                 const float fv = __fsub_rn(vi, float(v0));
                                 const float val = jwb * __ldg(&col[z]);

@@ -47,8 +47,38 @@ __device__ __forceinline__ RowLine row_line(float U, float h, float zpv, float v
 
 __device__ __forceinline__ float row_at(const RowLine& r, float zf) { return fmaf(zf, r.mdv, r.c0); }
 
-// A row coordinate is inside the detector when 0 <= vi <= H - 1.1
-// (the v bounds of :927-928 and :1011 expressed on vi).
-__device__ __forceinline__ bool row_ok(float vi, float vi_hi) { return vi >= 0.0f && vi <= vi_hi; }
+// Whether a voxel falls inside the detector's rows, decided exactly as the
+// reference decides it (:926-928, :1008-1011): v = (z + h) U rounded in float
+// and kept when lbV <= v <= ubV, with zw the voxel's world z. The row line
+// above gives the row and its weight; near the first and last row its single
+// rounding can land on the other side of a bound that the reference's v hits
+// exactly (a voxel whose v equals ubV, row 0), so membership is taken from
+// here. A kept voxel's row line value then lies within rounding of [0, H-1.1],
+// and int() of it still names rows inside the detector.
+__device__ __forceinline__ bool v_inside(float zw, float h, float U, float lbV, float ubV) {
+    const float v = __fmul_rn(__fadd_rn(zw, h), U);
+    return v >= lbV && v <= ubV;
+}
+
+// The same decision for the n slices zs .. zs+n-1 of one column at once: v
+// grows with z (U > 0, vs > 0) and rounding keeps it monotone, so the kept
+// slices are one run [*ja, *jb] (local indices; empty when *ja > *jb). Its
+// ends are estimated from the continuous v and settled with v_inside's own
+// arithmetic (a step or two), instead of testing every slice.
+__device__ __forceinline__ void v_inside_run(int zs, int n, float zPre, float vs, float h, float U, float lbV,
+                                             float ubV, int* ja, int* jb) {
+    auto v = [&](int j) { return __fmul_rn(__fadd_rn(__fmul_rn(__fsub_rn(float(zs + j), zPre), vs), h), U); };
+    const float rv = 1.0f / vs, ru = 1.0f / U, base = zPre - float(zs);
+    // last j with v <= ubV
+    int b = int(floorf(fminf(fmaxf((ubV * ru - h) * rv + base, -1.0f), float(n - 1))));
+    while (b + 1 <= n - 1 && v(b + 1) <= ubV) ++b;
+    while (b >= 0 && v(b) > ubV) --b;
+    // first j with v >= lbV
+    int a = int(ceilf(fminf(fmaxf((lbV * ru - h) * rv + base, 0.0f), float(n))));
+    while (a - 1 >= 0 && v(a - 1) >= lbV) --a;
+    while (a <= n - 1 && v(a) < lbV) ++a;
+    *ja = a;
+    *jb = b;
+}
 
 }  // namespace ctb

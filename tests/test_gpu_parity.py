@@ -400,3 +400,21 @@ def test_emit_signals_off_silences_callbacks(tmp_path):
     v.setEmitSignals(True)
     v.reconstructVolume()
     assert seen and seen[-1] == 100.0
+
+
+@pytest.mark.parametrize("V,H,W,FCD", [(24, 20, 32, 120.0), (24, 20, 64, 240.0), (36, 18, 40, 90.0)])
+def test_row_bounds_decided_as_the_reference(oracle, V, H, W, FCD):
+    """Geometries where voxels of the first and last slices project exactly onto the detector's
+    row bounds (v == H/2 at 180 degrees): membership must follow the reference's own v test, else
+    whole rows of voxels gain or lose a boundary sample (filtered noise makes that visible)."""
+    rng = np.random.default_rng(V + H + W)
+    imgs = rng.integers(20000, 65535, size=(V, H, W)).astype(np.uint16)
+    angles = np.arange(V) * (360.0 / V)
+    det, grid = ops.detector(W, H, FCD)
+    raw = torch.from_numpy(imgs.astype(np.int32)).to(torch.uint16).cuda()
+    filt = ops.filter_projections(raw, det, L.RAMLAK, 1, L.FP32)
+    vol = ops.backproject(filt, angles, None, det, grid)
+    torch.cuda.synchronize()
+    og = oracle.ref_geom(W, H, FCD)
+    ref, _ = oracle.ref_reconstruct(imgs, angles, np.zeros(V), 1.0, oracle.RAMLAK, og)
+    assert rel_l2(vol.cpu().numpy().transpose(2, 1, 0), ref) < 1e-5

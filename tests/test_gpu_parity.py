@@ -418,3 +418,12 @@ def test_row_bounds_decided_as_the_reference(oracle, V, H, W, FCD):
     og = oracle.ref_geom(W, H, FCD)
     ref, _ = oracle.ref_reconstruct(imgs, angles, np.zeros(V), 1.0, oracle.RAMLAK, og)
     assert rel_l2(vol.cpu().numpy().transpose(2, 1, 0), ref) < 1e-5
+
+
+def test_smoke_entry_point():
+    """The build's own smoke check (one small reconstruction against the CPU oracle)."""
+    import sys
+    if ROOT not in sys.path:
+        sys.path.insert(0, ROOT)
+    import __graft_entry__
+    __graft_entry__.smoke()

@@ -427,3 +427,40 @@ def test_smoke_entry_point():
         sys.path.insert(0, ROOT)
     import __graft_entry__
     __graft_entry__.smoke()
+
+
+def _random_case(k):
+    rng = np.random.default_rng(1000 + k)
+    W = int(rng.integers(16, 97))
+    H = int(rng.integers(8, 65))
+    FCD = float(rng.uniform(2.0, 6.0) * W)
+    V = int(rng.integers(4, 41))
+    angles = np.arange(V) * (360.0 / V) if k % 2 == 0 else np.sort(rng.uniform(0, 360, V))
+    uoff = float(rng.choice([0.0, 2.5, -1.75]))
+    heights = rng.uniform(-2.0, 2.0, V) if k % 3 == 0 else np.zeros(V)
+    heights = heights - heights.mean()
+    lo = rng.uniform(0.0, 0.4, 3)
+    hi = rng.uniform(0.6, 1.0, 3)
+    rel = (lo[0], hi[0], lo[1], hi[1], lo[2], hi[2]) if k % 4 == 1 else (0, 1, 0, 1, 0, 1)
+    ft = int(k % 3)
+    imgs = rng.integers(2000, 65535, size=(V, H, W)).astype(np.uint16)
+    return W, H, FCD, angles, uoff, heights, rel, ft, imgs
+
+
+@pytest.mark.parametrize("k", range(16))
+def test_random_geometries_match_reference_path(oracle, k):
+    """Seeded random detectors, orbits, u offsets, height offsets, sub-boxes and filters on noise
+    projections (the input on which any boundary decision that differs from the reference's
+    shows): the FP32 engine against the reference's CPU path restated."""
+    W, H, FCD, angles, uoff, heights, rel, ft, imgs = _random_case(k)
+    V = len(angles)
+    rel_c = oracle.clamp_bounds(*rel)
+    det, grid = ops.detector(W, H, FCD, u_offset=uoff, rel=rel)
+    raw = torch.from_numpy(imgs.astype(np.int32)).to(torch.uint16).cuda()
+    filt = ops.filter_projections(raw, det, ft, 1, L.FP32)
+    vol = ops.backproject(filt, angles, heights, det, grid)
+    torch.cuda.synchronize()
+    og = oracle.ref_geom(W, H, FCD, uoff, rel=rel_c)
+    ref, _ = oracle.ref_reconstruct(imgs, angles, heights, 1.0, ft, og)
+    err = rel_l2(vol.cpu().numpy().transpose(2, 1, 0), ref)
+    assert err < 2e-5, err

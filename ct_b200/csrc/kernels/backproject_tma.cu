@@ -80,6 +80,39 @@ template <> __device__ __forceinline__ float sval<float>(float v) { return v; }
 template <> __device__ __forceinline__ float sval<__half>(__half v) { return __half2float(v); }
 template <> __device__ __forceinline__ float sval<__nv_bfloat16>(__nv_bfloat16 v) { return __bfloat162float(v); }
 
+// The fast column loop on pairs of voxels (j, j + 1) with the FP32x2
+// instructions of sm_100 (one issue slot for two lanes' worth of FFMA/FADD).
+// Same operations and roundings as the scalar loop, so the sums are
+// bit-identical: the row floor is taken by adding 1.5 * 2^23 rounded toward
+// zero (exact for 0 <= vi < 2^22; the caller guarantees vi >= 0.5), whose low
+// bits are the row index and whose difference from the magic is float(v0);
+// subtractions are FMAs with a -1 factor (one rounding, as a subtraction).
+template <typename T, int ZC>
+__device__ __forceinline__ void column_pairs(const T* col, int BU, const float* zf, float mdv, float c0, float fu,
+                                             float w, float* acc) {
+    constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
+    const float2 mdv2 = make_float2(mdv, mdv), c02 = make_float2(c0, c0);
+    const float2 fu2 = make_float2(fu, fu), w2 = make_float2(w, w);
+    const float2 m1 = make_float2(-1.0f, -1.0f), mg = make_float2(kMagic, kMagic);
+#pragma unroll
+    for (int j = 0; j < ZC; j += 2) {
+        const float2 vi = __ffma2_rn(make_float2(zf[j], zf[j + 1]), mdv2, c02);
+        const float2 sm = __fadd2_rz(vi, mg);
+        const float2 nfl = __ffma2_rn(sm, m1, mg);   // -float(floor(vi))
+        const float2 fv = __fadd2_rn(vi, nfl);
+        const T* ra = col + (__float_as_int(sm.x) - 0x4B400000) * BU;
+        const T* rb = col + (__float_as_int(sm.y) - 0x4B400000) * BU;
+        const float2 p00 = make_float2(sval(ra[0]), sval(rb[0])), p01 = make_float2(sval(ra[1]), sval(rb[1]));
+        const float2 p10 = make_float2(sval(ra[BU]), sval(rb[BU])), p11 = make_float2(sval(ra[BU + 1]), sval(rb[BU + 1]));
+        const float2 a = __ffma2_rn(fu2, __ffma2_rn(p00, m1, p01), p00);
+        const float2 c = __ffma2_rn(fu2, __ffma2_rn(p10, m1, p11), p10);
+        const float2 r = __ffma2_rn(fv, __ffma2_rn(a, m1, c), a);
+        const float2 s = __ffma2_rn(w2, r, make_float2(acc[j], acc[j + 1]));
+        acc[j] = s.x;
+        acc[j + 1] = s.y;
+    }
+}
+
 template <typename T> __device__ __forceinline__ float gval(const T* p);
 template <> __device__ __forceinline__ float gval<float>(const float* p) { return __ldg(p); }
 template <> __device__ __forceinline__ float gval<__half>(const __half* p) { return __half2float(__ldg(p)); }
@@ -269,18 +302,7 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                     // the per-voxel membership test, so this loop and the checked one take the same
                     // decisions
                     if (fminf(vf, vl) >= 0.5f && fmaxf(vf, vl) <= g.vi_hi - 0.5f) {
-#pragma unroll
-                        for (int j = 0; j < ZC; ++j) {
-                            const float vi = row_at(rl, zf[j]);
-                            const int v0 = int(vi);
-                            const float fv = __fsub_rn(vi, float(v0));
-                            const T* r0 = col + v0 * BU;
-                            const float p00 = sval(r0[0]), p01 = sval(r0[1]);
-                            const float p10 = sval(r0[BU]), p11 = sval(r0[BU + 1]);
-                            const float a = fmaf(fu, p01 - p00, p00);
-                            const float c = fmaf(fu, p11 - p10, p10);
-                            acc[j] = fmaf(w, fmaf(fv, c - a, a), acc[j]);
-                        }
+                        column_pairs<T, ZC>(col, BU, zf, rl.mdv, rl.c0, fu, w, acc);
                     } else {
                         int ja, jb;
                         v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);

@@ -481,8 +481,25 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     if (R >= 0.9 * D) return false;
     const double Umax = D / (D - R), dU = Umax * Umax / D;
     const double T = std::sqrt(std::pow((kTX - 1) * vs, 2) + std::pow((kTY - 1) * vs, 2));
-    const double tmax = R + std::fabs(g.uOff);
-    const double uext = Umax * T + tmax * dU * T;
+    // Width: with a tile centre at (s, t) in a view's frame (t including the
+    // detector offset), u = D t / (D - s) has gradient U (1, t U / D), U =
+    // D / (D - s), so the tile's corners (diagonal T) span at most
+    // T U sqrt(1 + (t U / D)^2) to first order; the second-order terms
+    // (|u_ss| = 2 |t| U^3 / D^2, |u_st| = U^2 / D) add at most
+    // (T/2)^2 (|u_ss| + 2 |u_st|) / 2. For each s the largest |t| within R
+    // of the axis is the worst; s is scanned finely (the extent changes by
+    // far less than 0.05 pixel between samples). Views whose footprint still
+    // does not fit are read through global memory by the kernel.
+    double uext = 0.0;
+    for (int i = 0; i <= 4096; ++i) {
+        const double s = R * (2.0 * i / 4096 - 1.0);
+        const double t = std::sqrt(std::max(0.0, R * R - s * s)) + std::fabs(g.uOff);
+        const double U = D / (D - s);
+        const double first = T * U * std::sqrt(1.0 + (t * U / D) * (t * U / D));
+        const double second = 0.125 * T * T * (2.0 * t * U * U * U / (D * D) + 2.0 * U * U / D);
+        uext = std::max(uext, first + second);
+    }
+    uext += 0.05;
     const double zabs =
         std::max(std::fabs((0 - g.zPre) * vs), std::fabs((g.Zs + ZC - 1 - g.zPre) * vs)) + hmax;
     const double vext = (ZC - 1) * vs * Umax + zabs * dU * T;

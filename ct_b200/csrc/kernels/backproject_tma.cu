@@ -88,8 +88,8 @@ template <> __device__ __forceinline__ float sval<__nv_bfloat16>(__nv_bfloat16 v
 // bits are the row index and whose difference from the magic is float(v0);
 // subtractions are FMAs with a -1 factor (one rounding, as a subtraction).
 template <typename T, int ZC>
-__device__ __forceinline__ void column_pairs(const T* col, int BU, const float* zf, float mdv, float c0, float fu,
-                                             float w, float* acc) {
+__device__ __forceinline__ void column_pairs(const T* col, const int BU, const float* zf, float mdv, float c0,
+                                             float fu, float w, float* acc) {
     constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
     const float2 mdv2 = make_float2(mdv, mdv), c02 = make_float2(c0, c0);
     const float2 fu2 = make_float2(fu, fu), w2 = make_float2(w, w);
@@ -503,16 +503,16 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     const double zabs =
         std::max(std::fabs((0 - g.zPre) * vs), std::fabs((g.Zs + ZC - 1 - g.zPre) * vs)) + hmax;
     const double vext = (ZC - 1) * vs * Umax + zabs * dU * T;
-    // Row stride. 16-bit texels: 64 bytes more than a multiple of 128, so two
-    // adjacent box rows sit 16 banks apart and a warp whose lanes sample one
-    // row pair within 32 texels never conflicts (measured 1 % faster on C3 than
-    // the odd-chunk rule). 32-bit texels: an odd number of 16-byte chunks
-    // (consecutive rows start in different banks; the 64-byte rule made the
-    // FP32 box larger and was 30 % slower there).
-    const int chunk = 16 / esize;
+    // Row stride: 64 bytes more than a multiple of 128, so two adjacent box
+    // rows sit 16 banks apart and a warp whose lanes sample one row pair
+    // within 16 banks' width never conflicts (C3, box 96 / 112 texels wide:
+    // FP16 1 % faster than an odd number of 16-byte chunks, FP32 7 %).
+    // Strides past 256 texels fall back to the odd-chunk rule (consecutive
+    // rows start in different banks) to keep the box small.
+    const int chunk = 16 / esize, per128 = 128 / esize, half = 64 / esize;
     int BU = int(std::ceil(uext)) + 12;
-    const int bu64 = (BU - 32 + 63) / 64 * 64 + 32;
-    if (esize == 2 && bu64 <= 256) {
+    const int bu64 = (BU - half + per128 - 1) / per128 * per128 + half;
+    if (bu64 <= 256) {
         BU = bu64;
     } else {
         BU = (BU + chunk - 1) / chunk * chunk;
@@ -522,7 +522,6 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     if (BU > 256 || BV > 256) return false;
     b->BU = BU;
     b->BV = BV;
-    const int per128 = 128 / esize;
     b->buf_elems = (BU * BV + per128 - 1) / per128 * per128;
     b->vi_hi = float(double(g.H) - 1 - 0.1);
     return true;

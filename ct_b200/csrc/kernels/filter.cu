@@ -367,6 +367,220 @@ __global__ void __launch_bounds__(1024) filter_kernel(const InT* __restrict__ ra
     fft_run<true, kFromSmem, kToOutput>(s, M, a.logM, tw, K, lt, TG, load, store);
 }
 
+// --------------------------------------- register four-step transform
+// For M = 16 L with L = 16 L2 (M = 512 ... 4096) a group of L threads owns one
+// row pair. Every thread keeps 16 complex values in registers and the
+// transform is three register passes joined by two shared-memory transposes:
+//   1. thread t:       16-point DFT over r of x[t + L r], times w_M^(t s)
+//   2. thread (s, t2): 16-point DFT over r of pass 1's values (t2 + L2 r, s),
+//                      times w_L^(t2 s2)
+//   3. thread (s, j):  for s2 = j + L2 q (q < 16 / L2) the L2-point DFT over t2,
+// which leaves X[s + 16 s2 + 256 k3] in registers (k3 < L2). The kernel
+// spectrum multiplies it there; the inverse runs the passes backwards with
+// conjugate factors and ends with thread t holding x[t + L r] again, so raw
+// rows are read and filtered rows written with the same coalesced pattern.
+// The exchange between passes 2 and 3 stays inside a warp. The paddings (HP
+// per 16-value row of the first transpose, 1 per s2 row and HP per s block of
+// the second) keep every shared-memory access at two wavefronts per warp, the
+// minimum for 8-byte elements. Three block barriers per row pair.
+template <int M> struct RF {
+    static constexpr int L = M / 16, L2 = L / 16, Q = 16 / L2;
+    static constexpr int HP = L2 / 2 > 0 ? L2 / 2 : 1;
+    static constexpr int SA = 16 * (L + HP);       // first transpose, float2 per group
+    static constexpr int SB = 16 * (L2 + 1) + HP;  // second transpose, float2 per s block
+    static constexpr int SG = SA + 16 * SB;        // float2 per group
+    static constexpr int G = 256 / L;              // row pairs per CTA of 256 threads
+    static_assert(M >= 512 && M <= 4096 && (M & (M - 1)) == 0, "register transform lengths");
+};
+
+__device__ __forceinline__ float2 cmul_conj(float2 a, float2 b) {
+    return make_float2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+
+// x times w16^m (forward: exp(-2 pi i m / 16); inverse: the conjugate)
+template <bool INV, int m>
+__device__ __forceinline__ float2 tw16(float2 x) {
+    constexpr float c1 = 0.92387953251128675613f, s1 = 0.38268343236508977173f;
+    // cos and sin of 2 pi m / 16 for m = 0 ... 9 (m = n1 k2 <= 9)
+    constexpr float cs[10] = {1.0f, c1, kSqrtHalf, s1, 0.0f, -s1, -kSqrtHalf, -c1, -1.0f, -c1};
+    constexpr float sn[10] = {0.0f, s1, kSqrtHalf, c1, 1.0f, c1, kSqrtHalf, s1, 0.0f, -s1};
+    static_assert(m >= 0 && m <= 9, "twiddle index");
+    if constexpr (m == 0) return x;
+    else if constexpr (m == 4) return rot90<INV>(x);
+    else {
+        const float c = cs[m], sv = sn[m];
+        return INV ? make_float2(x.x * c - x.y * sv, x.y * c + x.x * sv)
+                   : make_float2(x.x * c + x.y * sv, x.y * c - x.x * sv);
+    }
+}
+
+template <bool INV, int n1>
+__device__ __forceinline__ void tw16_row(float2* a) {
+    a[1] = tw16<INV, n1 * 1>(a[1]);
+    a[2] = tw16<INV, n1 * 2>(a[2]);
+    a[3] = tw16<INV, n1 * 3>(a[3]);
+}
+
+// 16-point DFT in registers, natural order in and out: n = n1 + 4 n2,
+// k = 4 k1 + k2; 4-point DFTs over n2, twiddles w16^(n1 k2), 4-point DFTs over n1.
+template <bool INV>
+__device__ __forceinline__ void dft16(float2* v) {
+    float2 a[4][4];
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) {
+        a[n1][0] = v[n1]; a[n1][1] = v[n1 + 4]; a[n1][2] = v[n1 + 8]; a[n1][3] = v[n1 + 12];
+        dft4<INV>(a[n1][0], a[n1][1], a[n1][2], a[n1][3]);
+    }
+    tw16_row<INV, 1>(a[1]);
+    tw16_row<INV, 2>(a[2]);
+    tw16_row<INV, 3>(a[3]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) {
+        dft4<INV>(a[0][k2], a[1][k2], a[2][k2], a[3][k2]);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1) v[4 * k1 + k2] = a[k1][k2];
+    }
+}
+
+template <int N, bool INV>
+__device__ __forceinline__ void dft_n(float2* v) {
+    if constexpr (N == 2) dft2<INV>(v);
+    else if constexpr (N == 4) dft4<INV>(v[0], v[1], v[2], v[3]);
+    else if constexpr (N == 8) dft8<INV>(v);
+    else dft16<INV>(v);
+}
+
+template <int M, typename InT, typename OutT>
+__global__ void __launch_bounds__(256, 3) filter_rf_kernel(const InT* __restrict__ raw, OutT* __restrict__ out,
+                                                           FilterArgs a, const float2* __restrict__ tw,
+                                                           const float* __restrict__ K) {
+    using C = RF<M>;
+    constexpr int L = C::L, L2 = C::L2, Q = C::Q;
+    extern __shared__ float2 smem[];
+    const int g = threadIdx.x / L, lt = threadIdx.x % L;
+    float2* sa = smem + g * C::SG;
+    const int W = a.W, H = a.H;
+    const int pairs = (H + 1) >> 1;
+    const long long q = (long long)blockIdx.x * C::G + g;
+    const bool active = q < a.n_views * pairs;
+    const long long view = active ? q / pairs : 0;
+    const int r0 = active ? int(q - view * pairs) * 2 : 0;
+    const bool has1 = active && r0 + 1 < H;
+    const InT* src = raw + (size_t)view * H * W + (size_t)r0 * W;
+    const float* wrow = a.wt + (size_t)r0 * W;
+
+    float2 v[16];
+    {
+        // all 64 loads of the thread (16 columns x 2 rows, samples and weights)
+        // are issued before any arithmetic
+        InT x0[16], x1[16];
+        float w0[16], w1[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int c = lt + L * r;
+            const bool in = active && c < W;
+            x0[r] = in ? src[c] : InT(0);
+            x1[r] = in && has1 ? src[W + c] : InT(0);
+            w0[r] = in ? __ldg(wrow + c) : 0.0f;
+            w1[r] = in && has1 ? __ldg(wrow + W + c) : 0.0f;
+        }
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int c = lt + L * r;
+            float2 z = make_float2(0.f, 0.f);
+            if (active && c < W) {
+                z.x = __fmul_rn(log_part(raw_value(&x0[r], a), a), w0[r]);
+                if (has1) z.y = __fmul_rn(log_part(raw_value(&x1[r], a), a), w1[r]);
+            }
+            v[r] = z;
+        }
+    }
+    // pass 1
+    dft16<false>(v);
+#pragma unroll
+    for (int s = 1; s < 16; ++s) v[s] = cmul(v[s], __ldg(&tw[lt * s]));
+#pragma unroll
+    for (int s = 0; s < 16; ++s) sa[s * (L + C::HP) + lt] = v[s];
+    __syncthreads();
+    // pass 2
+    const int ps = lt / L2, t2 = lt % L2;
+    float2* bs = sa + C::SA + ps * C::SB;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = sa[ps * (L + C::HP) + t2 + L2 * r];
+    dft16<false>(v);
+#pragma unroll
+    for (int s2 = 1; s2 < 16; ++s2) v[s2] = cmul(v[s2], __ldg(&tw[16 * t2 * s2]));
+#pragma unroll
+    for (int s2 = 0; s2 < 16; ++s2) bs[s2 * (L2 + 1) + t2] = v[s2];
+    __syncwarp();
+    // pass 3, the kernel spectrum, inverse pass 3
+    {
+        float2 u[Q][L2];
+#pragma unroll
+        for (int qq = 0; qq < Q; ++qq)
+#pragma unroll
+            for (int k = 0; k < L2; ++k) u[qq][k] = bs[(t2 + L2 * qq) * (L2 + 1) + k];
+#pragma unroll
+        for (int qq = 0; qq < Q; ++qq) {
+            dft_n<L2, false>(u[qq]);
+#pragma unroll
+            for (int k3 = 0; k3 < L2; ++k3) {
+                const float kf = __ldg(&K[ps + 16 * (t2 + L2 * qq) + 256 * k3]);
+                u[qq][k3] = make_float2(u[qq][k3].x * kf, u[qq][k3].y * kf);
+            }
+            dft_n<L2, true>(u[qq]);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int qq = 0; qq < Q; ++qq)
+#pragma unroll
+            for (int k = 0; k < L2; ++k) bs[(t2 + L2 * qq) * (L2 + 1) + k] = u[qq][k];
+        __syncwarp();
+    }
+    // inverse pass 2
+#pragma unroll
+    for (int s2 = 0; s2 < 16; ++s2) v[s2] = bs[s2 * (L2 + 1) + t2];
+#pragma unroll
+    for (int s2 = 1; s2 < 16; ++s2) v[s2] = cmul_conj(v[s2], __ldg(&tw[16 * t2 * s2]));
+    dft16<true>(v);
+    __syncthreads();  // every warp has read its pass-2 values from sa
+#pragma unroll
+    for (int r = 0; r < 16; ++r) sa[ps * (L + C::HP) + t2 + L2 * r] = v[r];
+    __syncthreads();
+    // inverse pass 1 and the filtered rows
+#pragma unroll
+    for (int s = 0; s < 16; ++s) v[s] = sa[s * (L + C::HP) + lt];
+#pragma unroll
+    for (int s = 1; s < 16; ++s) v[s] = cmul_conj(v[s], __ldg(&tw[lt * s]));
+    dft16<true>(v);
+    const size_t obase = (size_t)view * H * a.out_pitch + (size_t)r0 * a.out_pitch;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        const int c = lt + L * r;
+        if (active && c < W) {
+            out[obase + c] = to_store<OutT>(v[r].x * a.store_scale);
+            if (has1) out[obase + a.out_pitch + c] = to_store<OutT>(v[r].y * a.store_scale);
+        }
+    }
+}
+
+template <int M, typename InT, typename OutT>
+int launch_rf(const InT* raw, OutT* out, const FilterArgs& a, const float2* tw, const float* K, cudaStream_t s) {
+    using C = RF<M>;
+    const long long pairs = a.n_views * ((a.H + 1) / 2);
+    const long long blocks = (pairs + C::G - 1) / C::G;
+    if (blocks <= 0) return CTB_OK;
+    if (blocks > 0x7fffffffLL) {
+        set_global_error("filter: too many rows for one launch");
+        return CTB_ERR_UNSUPPORTED;
+    }
+    const size_t smem = size_t(C::G) * C::SG * sizeof(float2);
+    auto kern = filter_rf_kernel<M, InT, OutT>;
+    if (const int st = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return st;
+    kern<<<unsigned(blocks), 256, smem, s>>>(raw, out, a, tw, K);
+    return cuda_status(cudaGetLastError(), "filter_rf_kernel launch");
+}
+
 template <typename InT, typename OutT>
 int launch_typed(const InT* raw, OutT* out, const FilterArgs& a, const float2* tw, const float* K,
                  cudaStream_t s) {
@@ -382,6 +596,14 @@ int launch_typed(const InT* raw, OutT* out, const FilterArgs& a, const float2* t
         return CTB_ERR_UNSUPPORTED;
     }
     const bool tab = a.wt != nullptr;
+    if (tab) {
+        switch (a.M) {
+            case 512: return launch_rf<512>(raw, out, a, tw, K, s);
+            case 1024: return launch_rf<1024>(raw, out, a, tw, K, s);
+            case 2048: return launch_rf<2048>(raw, out, a, tw, K, s);
+            case 4096: return launch_rf<4096>(raw, out, a, tw, K, s);
+        }
+    }
     auto kern = tab ? filter_kernel<InT, OutT, true> : filter_kernel<InT, OutT, false>;
     if (smem > 48 * 1024)
         if (const int st = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return st;

@@ -379,17 +379,19 @@ __global__ void __launch_bounds__(1024) filter_kernel(const InT* __restrict__ ra
 // spectrum multiplies it there; the inverse runs the passes backwards with
 // conjugate factors and ends with thread t holding x[t + L r] again, so raw
 // rows are read and filtered rows written with the same coalesced pattern.
-// The exchange between passes 2 and 3 stays inside a warp. The paddings (HP
-// per 16-value row of the first transpose, 1 per s2 row and HP per s block of
-// the second) keep every shared-memory access at two wavefronts per warp, the
-// minimum for 8-byte elements. Three block barriers per row pair.
+// The exchange between passes 2 and 3 stays inside a warp. The paddings (L2
+// per 16-value row of the first transpose, 1 per s2 row and L2 per s block of
+// the second) keep every shared-memory access at two wavefronts per warp (one
+// per half-warp, the minimum for 8-byte elements). Three block barriers per
+// row pair; four where the second transpose reuses the first one's space so
+// that three CTAs fit an SM.
 template <int M> struct RF {
     static constexpr int L = M / 16, L2 = L / 16, Q = 16 / L2;
-    static constexpr int HP = L2 / 2 > 0 ? L2 / 2 : 1;
-    static constexpr int SA = 16 * (L + HP);       // first transpose, float2 per group
-    static constexpr int SB = 16 * (L2 + 1) + HP;  // second transpose, float2 per s block
-    static constexpr int SG = SA + 16 * SB;        // float2 per group
+    static constexpr int SA = 16 * (L + L2);       // first transpose, float2 per group
+    static constexpr int SB = 16 * (L2 + 1) + L2;  // second transpose, float2 per s block
     static constexpr int G = 256 / L;              // row pairs per CTA of 256 threads
+    static constexpr bool ALIAS = 3 * (size_t(G) * (SA + 16 * SB) * 8 + 1024) > 227 * 1024;
+    static constexpr int SG = ALIAS ? (SA > 16 * SB ? SA : 16 * SB) : SA + 16 * SB;  // float2 per group
     static_assert(M >= 512 && M <= 4096 && (M & (M - 1)) == 0, "register transform lengths");
 };
 
@@ -470,7 +472,24 @@ __global__ void __launch_bounds__(256, 3) filter_rf_kernel(const InT* __restrict
     const float* wrow = a.wt + (size_t)r0 * W;
 
     float2 v[16];
-    {
+    if (has1 && W == M) {
+        // whole row pair inside the detector: no per-column tests; the weights
+        // of the second row are loaded after the first row is done
+        InT x0[16], x1[16];
+        float wv[16];
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            x0[r] = src[lt + L * r];
+            x1[r] = src[W + lt + L * r];
+            wv[r] = __ldg(wrow + lt + L * r);
+        }
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r].x = __fmul_rn(log_part(raw_value(&x0[r], a), a), wv[r]);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) wv[r] = __ldg(wrow + W + lt + L * r);
+#pragma unroll
+        for (int r = 0; r < 16; ++r) v[r].y = __fmul_rn(log_part(raw_value(&x1[r], a), a), wv[r]);
+    } else {
         // all 64 loads of the thread (16 columns x 2 rows, samples and weights)
         // are issued before any arithmetic
         InT x0[16], x1[16];
@@ -500,16 +519,17 @@ __global__ void __launch_bounds__(256, 3) filter_rf_kernel(const InT* __restrict
 #pragma unroll
     for (int s = 1; s < 16; ++s) v[s] = cmul(v[s], __ldg(&tw[lt * s]));
 #pragma unroll
-    for (int s = 0; s < 16; ++s) sa[s * (L + C::HP) + lt] = v[s];
+    for (int s = 0; s < 16; ++s) sa[s * (L + L2) + lt] = v[s];
     __syncthreads();
     // pass 2
     const int ps = lt / L2, t2 = lt % L2;
-    float2* bs = sa + C::SA + ps * C::SB;
+    float2* bs = sa + (C::ALIAS ? 0 : C::SA) + ps * C::SB;
 #pragma unroll
-    for (int r = 0; r < 16; ++r) v[r] = sa[ps * (L + C::HP) + t2 + L2 * r];
+    for (int r = 0; r < 16; ++r) v[r] = sa[ps * (L + L2) + t2 + L2 * r];
     dft16<false>(v);
 #pragma unroll
     for (int s2 = 1; s2 < 16; ++s2) v[s2] = cmul(v[s2], __ldg(&tw[16 * t2 * s2]));
+    if (C::ALIAS) __syncthreads();  // the second transpose overwrites the first
 #pragma unroll
     for (int s2 = 0; s2 < 16; ++s2) bs[s2 * (L2 + 1) + t2] = v[s2];
     __syncwarp();
@@ -545,11 +565,11 @@ __global__ void __launch_bounds__(256, 3) filter_rf_kernel(const InT* __restrict
     dft16<true>(v);
     __syncthreads();  // every warp has read its pass-2 values from sa
 #pragma unroll
-    for (int r = 0; r < 16; ++r) sa[ps * (L + C::HP) + t2 + L2 * r] = v[r];
+    for (int r = 0; r < 16; ++r) sa[ps * (L + L2) + t2 + L2 * r] = v[r];
     __syncthreads();
     // inverse pass 1 and the filtered rows
 #pragma unroll
-    for (int s = 0; s < 16; ++s) v[s] = sa[s * (L + C::HP) + lt];
+    for (int s = 0; s < 16; ++s) v[s] = sa[s * (L + L2) + lt];
 #pragma unroll
     for (int s = 1; s < 16; ++s) v[s] = cmul_conj(v[s], __ldg(&tw[lt * s]));
     dft16<true>(v);

@@ -556,7 +556,9 @@ def run_ours(args):
                 "traffic_unit": "DRAM bytes per backprojection launch (one slab)",
                 "algorithmic_bytes_per_launch": 8.0 * X * Y * slab * V,
                 "peak_basis": f"{sm_count} SMs x {clock_mhz:.0f} MHz (median sampled) x 32 lanes / 4 texel loads"}
-    roofline_filter = {"bound": "hbm", "kernel": "filter_kernel", "achieved": filt_gbs, "peak": peaks["hbm_gbs"],
+    fft_len = W if W & (W - 1) == 0 else 1 << (2 * W - 2).bit_length()   # transform length of the row filter
+    filt_kernel = "filter_rf_kernel" if 512 <= fft_len <= 4096 else "filter_kernel"
+    roofline_filter = {"bound": "hbm", "kernel": filt_kernel, "achieved": filt_gbs, "peak": peaks["hbm_gbs"],
                        "unit": "GB/s", "frac": filt_gbs / peaks["hbm_gbs"], "peak_kind": peak_kind,
                        "algorithmic_bytes_per_launch": V * H * W * (bytes_px_in + bytes_px_out)}
     launches_per_step = 1 + 2 * len(slabs)   # filter + (view table + backprojection) per slab

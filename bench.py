@@ -44,8 +44,8 @@ FILTERS = {"ramlak": 0, "shepplogan": 1, "hann": 2}
 
 # DRAM bytes (read + write) of one backprojection launch per voxel-view update, from one
 # ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of a C3 slab launch
-# (1024 x 1024 x 128 voxels x 1440 views of 2048^2, FP16): 196.6 GB / 1.93e11 updates
-BP_DRAM_BYTES_PER_UPDATE = {"c3": 196.59e9 / (1024 * 1024 * 128 * 1440)}
+# (1024 x 1024 x 128 voxels x 1440 views of 2048^2, FP16): 173.2 GB / 1.93e11 updates
+BP_DRAM_BYTES_PER_UPDATE = {"c3": (172.619e9 + 0.546e9) / (1024 * 1024 * 128 * 1440)}
 
 
 # --------------------------------------------------------------------- clocks

@@ -155,7 +155,7 @@ DeviceWork::~DeviceWork() {
         cudaStreamDestroy(s_down);
     }
     for (DevBuf* b : {&d_filtered, &d_ring, &d_views, &d_angles, &d_heights, &d_tw, &d_K, &d_slab[0], &d_slab[1],
-                      &d_conv[0], &d_conv[1]})
+                      &d_slab[2], &d_conv[0], &d_conv[1], &d_conv[2]})
         b->release();
 }
 
@@ -743,10 +743,12 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         cudaMemGetInfo(&freeb, &total);
         const size_t spare = spare_mb_ << 20;
         auto need = [&](int sl) {
-            return view_filt * V + 3 * view_raw * chunk + 2 * plane * sl * 4 * (convert ? 2 : 1) + 64 * V +
+            const size_t nb = std::min<size_t>(3, (Zw + sl - 1) / sl);
+            return view_filt * V + 3 * view_raw * chunk + nb * plane * sl * 4 * (convert ? 2 : 1) + 64 * V +
                    size_t(M) * 12;
         };
-        const size_t have = w.d_filtered.bytes + w.d_ring.bytes + w.d_slab[0].bytes * 2 + w.d_conv[0].bytes * 2;
+        size_t have = w.d_filtered.bytes + w.d_ring.bytes;
+        for (int b = 0; b < 3; ++b) have += w.d_slab[b].bytes + w.d_conv[b].bytes;
         while (slab > 16 && need(slab) > freeb + have - std::min(freeb + have, spare)) slab = std::max(16, slab / 2);
         if (need(slab) + spare > freeb + have)
             return fail(CTB_ERR_ALLOC,
@@ -761,7 +763,21 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         (st = w.d_heights.ensure(sizeof(double) * V, "height offsets")) ||
         (st = w.d_tw.ensure(sizeof(float2) * M, "twiddles")) || (st = w.d_K.ensure(sizeof(float) * M, "filter")))
         return fail(st, global_error());
-    for (int b = 0; b < 2; ++b) {
+    // Slab boundaries: slabs of `slab` slices, and a last one of 32 slices cut
+    // from a full-height last slab, so that the download no backprojection
+    // hides is short.
+    std::vector<int> zbound;
+    for (int z = z_lo; z < z_hi; z += slab) zbound.push_back(z);
+    zbound.push_back(z_hi);
+    if (zbound.size() >= 3 && zbound[zbound.size() - 1] - zbound[zbound.size() - 2] >= 64)
+        zbound.insert(zbound.end() - 1, z_hi - 32);
+    const int nslabs = int(zbound.size()) - 1;
+    // device slab buffers: the first `pre` slabs are backprojected while the
+    // views arrive (the upload alone would leave the GPU idle), a third buffer
+    // lets the next slab start before the first one has gone to the host
+    const int nbufs = std::min(3, nslabs);
+    const int pre = std::min(2, nslabs);
+    for (int b = 0; b < nbufs; ++b) {
         if ((st = w.d_slab[b].ensure(sizeof(float) * plane * slab, "volume slab"))) return fail(st, global_error());
         if (convert && (st = w.d_conv[b].ensure(sizeof(float) * plane * slab, "layout slab")))
             return fail(st, global_error());
@@ -773,10 +789,9 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
                 return fail(CTB_ERR_ALLOC, "Pinned staging memory could not be allocated.");
 
     // ---- events
-    cudaEvent_t ev_up[3], ev_free[3], ev_bp[2], ev_down[2], e_f0, e_f1, e_b0, e_b1;
+    cudaEvent_t ev_up[3], ev_free[3], ev_bp[3], ev_down[3], e_f0, e_f1, e_b0, e_b1;
     const int nchunks = (V + chunk - 1) / chunk;
-    const int nslabs = (Zw + slab - 1) / slab;
-    std::vector<cudaEvent_t> tf(2 * nchunks), tb(2 * (nslabs + nchunks));
+    std::vector<cudaEvent_t> tf(2 * nchunks), tb(2 * (nslabs + pre * nchunks));
     for (auto& e : tf) cudaEventCreate(&e);
     for (auto& e : tb) cudaEventCreate(&e);
     for (auto& e : ev_up) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
@@ -816,8 +831,9 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     // the ring slots start free
     for (auto& e : ev_free) cudaEventRecord(e, w.s_comp);
 
-    // ---- upload + filter; slab 0 is backprojected chunk by chunk as the views
-    // arrive, so the host-to-device transfer overlaps with its backprojection
+    // ---- upload + filter; the first `pre` slabs are backprojected chunk by
+    // chunk as the views arrive, so the host-to-device transfer overlaps with
+    // their backprojection
     const bool in_pinned = is_pinned(images_);
     auto slab_geom = [&](int zb, int ze) {
         ProjGeom g = proj_geom(det_, grid_, zb, ze, load_scale);
@@ -825,7 +841,8 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         g.view_stride = (long long)pitch * H;
         return g;
     };
-    const ProjGeom g0 = slab_geom(z_lo, std::min(z_hi, z_lo + slab));
+    ProjGeom gpre[2];
+    for (int p = 0; p < pre; ++p) gpre[p] = slab_geom(zbound[p], zbound[p + 1]);
     int nb_ev = 0;  // backprojection event pairs used
     cudaEventRecord(e_f0, w.s_comp);
     int slot = 0;
@@ -854,12 +871,14 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
             return cuda_fail("filter launch");
         cudaEventRecord(tf[2 * (c0 / chunk) + 1], w.s_comp);
         cudaEventRecord(ev_free[slot], w.s_comp);
-        cudaEventRecord(tb[2 * nb_ev], w.s_comp);
-        if (backproject_launch(fdst, store_, (const float4*)w.d_views.p + c0, n, g0, hmax, (float*)w.d_slab[0].p,
-                               c0 > 0, w.s_comp))
-            return cuda_fail("backprojection launch");
-        cudaEventRecord(tb[2 * nb_ev + 1], w.s_comp);
-        ++nb_ev;
+        for (int p = 0; p < pre; ++p) {
+            cudaEventRecord(tb[2 * nb_ev], w.s_comp);
+            if (backproject_launch(fdst, store_, (const float4*)w.d_views.p + c0, n, gpre[p], hmax,
+                                   (float*)w.d_slab[p].p, c0 > 0, w.s_comp))
+                return cuda_fail("backprojection launch");
+            cudaEventRecord(tb[2 * nb_ev + 1], w.s_comp);
+            ++nb_ev;
+        }
         if (!in_pinned) cudaStreamSynchronize(w.s_copy);
     }
     cudaEventRecord(e_f1, w.s_comp);
@@ -867,11 +886,10 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     // ---- backprojection per slab + layout + download
     cudaEventRecord(e_b0, w.s_comp);
     auto host_copy = [&](int k) {
-        // pageable output: staged slab k -> final position
-        const int b = k % 2;
-        const int zb = z_lo + k * slab, zs = std::min(slab, z_hi - zb);
-        cudaEventSynchronize(ev_down[b]);
-        const float* src = (const float*)w.h_stage[b].p;
+        // pageable output: staged slab k (staging buffer k % 2) -> final position
+        const int zb = zbound[k], zs = zbound[k + 1] - zb;
+        cudaEventSynchronize(ev_down[k % nbufs]);
+        const float* src = (const float*)w.h_stage[k % 2].p;
         if (order == CTB_Z_FASTEST) {
             parallel_for(plane, [&](size_t i) {
                 std::memcpy(out + i * Z + zb, src + i * zs, sizeof(float) * zs);
@@ -887,10 +905,10 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     };
     for (int k = 0; k < nslabs; ++k) {
         if (stop_) { cuda_fail("stop"); return fail(CTB_INTERRUPTED, "User interrupted. Stopping."); }
-        const int b = k % 2;
-        const int zb = z_lo + k * slab, ze = std::min(z_hi, zb + slab), zs = ze - zb;
-        if (k >= 2) cudaStreamWaitEvent(w.s_comp, ev_down[b], 0);
-        if (k > 0) {  // slab 0 was backprojected during the upload
+        const int b = k % nbufs;
+        const int zb = zbound[k], ze = zbound[k + 1], zs = ze - zb;
+        if (k >= nbufs) cudaStreamWaitEvent(w.s_comp, ev_down[b], 0);
+        if (k >= pre) {  // the first slabs were backprojected during the upload
             const ProjGeom g = slab_geom(zb, ze);
             cudaEventRecord(tb[2 * nb_ev], w.s_comp);
             if (backproject_launch(w.d_filtered.p, store_, (const float4*)w.d_views.p, V, g, hmax,
@@ -916,15 +934,16 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
                 ce = cudaMemcpyAsync(out + size_t(zb) * plane, src, sizeof(float) * plane * zs,
                                      cudaMemcpyDeviceToHost, w.s_down);
         } else {
-            if (k >= 2) host_copy(k - 2);  // frees staging buffer b
-            ce = cudaMemcpyAsync(w.h_stage[b].p, src, sizeof(float) * plane * zs, cudaMemcpyDeviceToHost, w.s_down);
+            if (k >= 2) host_copy(k - 2);  // frees staging buffer k % 2
+            ce = cudaMemcpyAsync(w.h_stage[k % 2].p, src, sizeof(float) * plane * zs, cudaMemcpyDeviceToHost,
+                                 w.s_down);
         }
         if (ce != cudaSuccess) return cuda_fail("volume download");
         cudaEventRecord(ev_down[b], w.s_down);
         // previews read the context's own volume up to the previous slab, which
         // has landed by now (waiting for this one would stall the next launch)
         const bool preview = previews() && out == static_cast<float*>(volume_.p) && out_pinned && k >= 1;
-        if (preview) cudaEventSynchronize(ev_down[(k - 1) % 2]);
+        if (preview) cudaEventSynchronize(ev_down[(k - 1) % nbufs]);
         worker_progress(w, double(k + 1) / double(nslabs), preview ? out : nullptr);
     }
     cudaEventRecord(e_b1, w.s_comp);
@@ -948,7 +967,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         float t = 0;
         cudaEventElapsedTime(&t, tb[2 * i], tb[2 * i + 1]);
         b_ms += t;
-        if (i < nchunks) bp0_ms += t;
+        if (i < pre * nchunks) bp0_ms += t;
     }
     cudaEventElapsedTime(&tail_ms, e_b0, e_b1);
     cleanup();

@@ -43,7 +43,7 @@ struct HostBuf {
 struct DeviceWork {
     int device = 0;
     cudaStream_t s_copy = nullptr, s_comp = nullptr, s_down = nullptr;
-    DevBuf d_filtered, d_ring, d_views, d_angles, d_heights, d_tw, d_K, d_slab[2], d_conv[2];
+    DevBuf d_filtered, d_ring, d_views, d_angles, d_heights, d_tw, d_K, d_slab[3], d_conv[3];
     HostBuf h_stage[2];
     int tables_key[3] = {-1, -1, -1};  // W, pad, filter of the cached tables
     // outcome of the last run

@@ -846,6 +846,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     int nb_ev = 0;  // backprojection event pairs used
     cudaEventRecord(e_f0, w.s_comp);
     int slot = 0;
+    int bp_from = 0;  // first view not yet backprojected into the early slabs
     for (int c0 = 0; c0 < V; c0 += chunk, slot = (slot + 1) % 3) {
         if (stop_) { cuda_fail("stop"); return fail(CTB_INTERRUPTED, "User interrupted. Stopping."); }
         const int n = std::min(chunk, V - c0);
@@ -871,17 +872,26 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
             return cuda_fail("filter launch");
         cudaEventRecord(tf[2 * (c0 / chunk) + 1], w.s_comp);
         cudaEventRecord(ev_free[slot], w.s_comp);
-        for (int p = 0; p < pre; ++p) {
-            cudaEventRecord(tb[2 * nb_ev], w.s_comp);
-            if (backproject_launch(fdst, store_, (const float4*)w.d_views.p + c0, n, gpre[p], hmax,
-                                   (float*)w.d_slab[p].p, c0 > 0, w.s_comp))
-                return cuda_fail("backprojection launch");
-            cudaEventRecord(tb[2 * nb_ev + 1], w.s_comp);
-            ++nb_ev;
+        // the early slabs take the views of every two chunks in one launch
+        // (C3, 32 views per chunk: 1 % faster end to end than every chunk, 4 %
+        // slower with four chunks)
+        constexpr int kBpGroup = 2;
+        if ((c0 / chunk) % kBpGroup == kBpGroup - 1 || c0 + n == V) {
+            for (int p = 0; p < pre; ++p) {
+                cudaEventRecord(tb[2 * nb_ev], w.s_comp);
+                if (backproject_launch((const char*)w.d_filtered.p + size_t(bp_from) * view_filt, store_,
+                                       (const float4*)w.d_views.p + bp_from, c0 + n - bp_from, gpre[p], hmax,
+                                       (float*)w.d_slab[p].p, bp_from > 0, w.s_comp))
+                    return cuda_fail("backprojection launch");
+                cudaEventRecord(tb[2 * nb_ev + 1], w.s_comp);
+                ++nb_ev;
+            }
+            bp_from = c0 + n;
         }
         if (!in_pinned) cudaStreamSynchronize(w.s_copy);
     }
     cudaEventRecord(e_f1, w.s_comp);
+    const int nb_early = nb_ev;  // backprojection launches of the upload phase
 
     // ---- backprojection per slab + layout + download
     cudaEventRecord(e_b0, w.s_comp);
@@ -967,7 +977,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         float t = 0;
         cudaEventElapsedTime(&t, tb[2 * i], tb[2 * i + 1]);
         b_ms += t;
-        if (i < pre * nchunks) bp0_ms += t;
+        if (i < nb_early) bp0_ms += t;
     }
     cudaEventElapsedTime(&tail_ms, e_b0, e_b1);
     cleanup();

@@ -9,23 +9,29 @@
 // voxels with u0 in {c-1, c} and v0 in {r-1, r} of
 //     w * (u0 == c ? 1-fu : fu) * (v0 == r ? 1-fv : fv) * vol.
 //
-// Ray-driven gather (deterministic, no atomics). A warp owns 256 detector rows
-// (eight per lane) of one detector column c of one view; everything that depends
-// only on (view, c) -- which voxel columns can reach c -- is shared by the
-// warp instead of being recomputed per lane:
+// Ray-driven gather (deterministic, no atomics). A warp owns a strip of kK = 8
+// adjacent detector columns c0 .. c0+7 and 256 rows (eight per lane) of one
+// view; everything that depends only on (view, strip) -- which voxel columns
+// can reach it -- is shared by the warp instead of being recomputed per lane:
 //  1. the warp walks the in-plane axis that is most perpendicular to the ray,
 //     32 positions at a time, one position per lane; each lane solves
-//     u(x, y) = c-1-W/2 and c+1-W/2 for the other axis (u is a ratio of linear
-//     functions) and gets a short range of candidate columns;
+//     u(x, y) = c0-1-W/2 and c0+8-W/2 for the other axis (u is a ratio of
+//     linear functions) and gets a short range of candidate columns;
 //  2. step by step through those ranges, each lane evaluates one candidate
 //     column with the very same FP32 expressions as the backprojector (so the
-//     discrete decisions u0, v0 and the masks agree bit for bit);
-//  3. the columns that reach c are broadcast one at a time (ballot + shuffles);
-//     the lanes then walk that column's slices whose rows reach the warp's 256
-//     rows, one slice each, and add each slice's two row weights into the
-//     warp's row accumulators in shared memory. Lanes that write in the same
-//     instruction hold slices far enough apart that their rows differ, and the
-//     order of the additions is fixed, so the result is deterministic.
+//     discrete decisions u0, v0 and the masks agree bit for bit), and for a
+//     column that reaches the strip (u0 in c0-1 .. c0+7) its run of slices
+//     inside the detector rows (the reference's v test, once per column);
+//  3. the columns that reach the strip are broadcast one at a time (ballot +
+//     shuffles); the lanes then walk that column's slices whose rows reach the
+//     warp's 256 rows, one slice each, and add each slice's shares to rows v0,
+//     v0+1 of detector columns u0, u0+1 (those inside the strip) in the warp's
+//     accumulators in shared memory. Lanes that write in the same instruction
+//     hold slices far enough apart that their rows differ, and the order of
+//     the additions is fixed, so the result is deterministic.
+// A voxel column is evaluated by one warp, or by two when u0 is the last
+// column of a strip (the share of u0+1 belongs to the next strip): 1.125
+// walks per voxel and view instead of the two of a warp per detector column.
 // The volume is read in a z-fastest copy so that a warp's lanes (consecutive
 // rows -> consecutive z) read contiguous memory.
 
@@ -36,31 +42,39 @@ namespace ctb {
 
 namespace {
 
-// a CTA: kFC detector columns (one warp each) x kFR * kRPL rows (kRPL per lane)
-constexpr int kFR = 32, kFC = 8, kRPL = 8;
+// a CTA: kFC warps, each kK detector columns x kFR * kRPL rows (kRPL per lane)
+constexpr int kFR = 32, kFC = 4, kK = 8, kRPL = 8;
+constexpr int kRows = kFR * kRPL, kStride = kRows + kRows / 32 + 1;
+__device__ __forceinline__ int rpos(int r) { return r + (r >> 5); }
 constexpr unsigned kAll = 0xffffffffu;
 
 __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__ volz,
                                                        const float4* __restrict__ views, ProjGeom g,
                                                        float* __restrict__ proj, int accumulate) {
-    __shared__ float s_rows[kFC][kFR * kRPL];  // per warp: rows R .. R + 255
+    // per warp: columns c0 .. c0+7, rows R .. R + 255; row r sits at
+    // r + r / 32, so lanes whose rows are 2 apart (slices one pixel apart) hit
+    // 32 different banks
+    __shared__ float s_rows[kFC][kK][kStride];
     const int lane = threadIdx.x;
-    const int R = blockIdx.x * (kFR * kRPL);  // first row of the warp
-    const int c = blockIdx.y * kFC + threadIdx.y;
-    float* srow = s_rows[threadIdx.y];
+    const int R = blockIdx.x * kRows;  // first row of the warp
+    const int cs0 = (blockIdx.y * kFC + threadIdx.y) * kK;  // first column of the strip
+    float(*sacc)[kStride] = s_rows[threadIdx.y];
     const int iv = blockIdx.z;
-    if (c >= g.W) return;  // whole warps leave together
+    if (cs0 >= g.W) return;  // whole warps leave together
     const float4 q = __ldg(&views[iv]);
     const float sn = q.x, cs = q.y, h = q.z;
     const float D = g.D;
-    const double Tlo = double(c - 1) - double(g.uPre), Thi = double(c + 1) - double(g.uPre);
+    const double Tlo = double(cs0 - 1) - double(g.uPre), Thi = double(cs0 + kK) - double(g.uPre);
     const bool x_major = fabsf(cs) >= fabsf(sn);
     const int np = x_major ? g.X : g.Y;
     const int ns = x_major ? g.Y : g.X;
     const float ppre = x_major ? g.xPre : g.yPre;
     const float spre = x_major ? g.yPre : g.xPre;
 #pragma unroll
-    for (int k = 0; k < kRPL; ++k) srow[lane + k * kFR] = 0.0f;
+    for (int k = 0; k < kK; ++k)
+#pragma unroll
+        for (int r = 0; r < kStride; r += kFR)
+            if (r + lane < kStride) sacc[k][r + lane] = 0.0f;
     __syncwarp();
     for (int ip0 = 0; ip0 < np; ip0 += 32) {
         // (1) candidate range of this lane's position
@@ -88,8 +102,8 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
         for (int st = 0; st < steps; ++st) {
             // (2) this lane's candidate column for this step
             bool hit = false;
-            float wb = 0.0f, mdv = 0.0f, c0 = 0.0f, inv = 0.0f, Uc = 0.0f;
-            int colidx = 0;
+            float wa = 0.0f, wb = 0.0f, mdv = 0.0f, c0 = 0.0f, inv = 0.0f;
+            int colidx = 0, ku = 0, ja = 0, jb = -1;
             if (st < cnt) {
                 const int is = i0 + st;
                 const int x = x_major ? ip : is, y = x_major ? is : ip;
@@ -102,80 +116,103 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                         const float ui = __fadd_rn(u, g.uPre);
                         const int u0 = int(ui);
                         const float fu = __fsub_rn(ui, float(u0));
-                        if (u0 == c || u0 + 1 == c) {
-                            hit = true;
-                            const float bu = u0 == c ? 1.0f - fu : fu;
+                        if (u0 >= cs0 - 1 && u0 <= cs0 + kK - 1) {
+                            v_inside_run(0, g.Zs, g.zPre, g.vs, h, U, g.lbV, g.ubV, &ja, &jb);
+                            hit = ja <= jb;
                             const float w = __fmul_rn(__fmul_rn(U, U), g.load_scale);
-                            wb = w * bu;
+                            wa = w * (1.0f - fu);  // to column u0
+                            wb = w * fu;           // to column u0 + 1
                             const RowLine rl = row_line(U, h, g.zpv, g.vs, g.vPre);
                             mdv = rl.mdv;
                             c0 = rl.c0;
                             inv = 1.0f / -rl.mdv;
-                            Uc = U;
                             colidx = x * g.Y + y;
+                            ku = u0 - cs0;
                         }
                     }
                 }
             }
-            // (3) every lane adds the voxels of each hit column that reach its row
+            // (3) every lane adds the voxels of each hit column that reach its rows
             unsigned mask = __ballot_sync(kAll, hit);
             while (mask) {
                 const int j = __ffs(mask) - 1;
                 mask &= mask - 1;
+                const float jwa = __shfl_sync(kAll, wa, j);
                 const float jwb = __shfl_sync(kAll, wb, j);
                 const RowLine rl{__shfl_sync(kAll, mdv, j), __shfl_sync(kAll, c0, j)};
                 const float jinv = __shfl_sync(kAll, inv, j);
                 const int jcol = __shfl_sync(kAll, colidx, j);
-                const float jU = __shfl_sync(kAll, Uc, j);
+                const int jku = __shfl_sync(kAll, ku, j);
+                const int jja = __shfl_sync(kAll, ja, j);
+                const int jjb = __shfl_sync(kAll, jb, j);
                 // slices whose rows can reach R-1 .. R+255: box z in
                 // ((c0-R-257)/dv, (c0-R+1)/dv], dv = -mdv > 0, widened by m for the
                 // rounding of vi, of the quotients and of 1/dv (together below inv/16
-                // for rows under 2^17); the exact row test below decides
+                // for rows under 2^17); the exact row test below decides. Only the
+                // slices inside the detector rows (ja .. jb) add.
                 const float m = 0.08f * jinv + 0.01f;
                 const float zbig = float(g.z_begin + g.Zs) + 2.0f;
-                const float zlo = (rl.c0 - float(R + kFR * kRPL) - 1.0f) * jinv - m;
+                const float zlo = (rl.c0 - float(R + kRows) - 1.0f) * jinv - m;
                 const float zhi = (rl.c0 - float(R) + 1.0f) * jinv + m;
-                const int z0 = max(0, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) + 1 - g.z_begin);
-                const int z1 = min(g.Zs - 1, int(floorf(fmaxf(fminf(zhi, zbig), -2.0f))) - g.z_begin);
+                const int z0 = max(jja, int(floorf(fminf(fmaxf(zlo, -2.0f), zbig))) + 1 - g.z_begin);
+                const int z1 = min(jjb, int(floorf(fmaxf(fminf(zhi, zbig), -2.0f))) - g.z_begin);
                 // lanes st slices apart: their rows differ by st * dv > 1.02, more than
                 // the rounding of two row coordinates (2^-6 for rows under 2^17), so
                 // the lanes of one instruction never share a row (at st >= Zs only
                 // lane 0 has a slice, so the cap keeps that true)
-                const int st = min(int(fminf(jinv, 1.0e7f) * 1.02f) + 1, max(1, g.Zs));
+                const int sst = min(int(fminf(jinv, 1.0e7f) * 1.02f) + 1, max(1, g.Zs));
                 const float* col = volz + (long long)jcol * g.Zs;
-                for (int zb = z0; zb <= z1; zb += kFR * st) {
-                    for (int q = 0; q < st; ++q) {
-                        const int z = zb + q + lane * st;
-                        int lr = -2;
-                        float ca = 0.0f, cb = 0.0f;
-                        if (z <= z1) {
-                            const float vi = row_at(rl, float(g.z_begin + z));
-                            const float zw = __fmul_rn(__fsub_rn(float(z), g.zPre), g.vs);
-                            if (v_inside(zw, h, jU, g.lbV, g.ubV)) {
-                                const int v0 = int(vi);
-                                const float fv = __fsub_rn(vi, float(v0));
-                                const float val = jwb * __ldg(&col[z]);
-                                lr = v0 - R;
-                                ca = (1.0f - fv) * val;  // to row v0
-                                cb = fv * val;           // to row v0 + 1
-                            }
-                        }
-                        if (lr >= 0 && lr < kFR * kRPL) srow[lr] += ca;
-                        __syncwarp();
-                        if (lr + 1 >= 0 && lr + 1 < kFR * kRPL) srow[lr + 1] += cb;
-                        __syncwarp();
+                const bool left = jku >= 0, right = jku + 1 < kK;
+                float* ca_row = sacc[left ? jku : 0];
+                float* cb_row = sacc[right ? jku + 1 : 0];
+                if (z0 > z1) continue;
+                // steps (zb, qq): z = zb + qq + lane * sst for zb = z0, z0 + 32 sst, ...
+                // and qq < sst; each step's slice value is loaded one step ahead
+                int zb = z0, qq = 0;
+                float vz_next = z0 + lane * sst <= z1 ? __ldg(&col[z0 + lane * sst]) : 0.0f;
+                while (zb <= z1) {
+                    const int z = zb + qq + lane * sst;
+                    const float vz = vz_next;
+                    if (++qq == sst) {
+                        qq = 0;
+                        zb += kFR * sst;
                     }
+                    const int zn = zb + qq + lane * sst;
+                    if (zb <= z1) vz_next = zn <= z1 ? __ldg(&col[zn]) : 0.0f;
+                    int lr = -2;
+                    float a0 = 0.0f, a1 = 0.0f, b0 = 0.0f, b1 = 0.0f;
+                    if (z <= z1) {
+                        const float vi = row_at(rl, float(g.z_begin + z));
+                        const int v0 = int(vi);
+                        const float fv = __fsub_rn(vi, float(v0));
+                        const float va = jwa * vz, vb = jwb * vz;
+                        lr = v0 - R;
+                        a0 = (1.0f - fv) * va;  // row v0, column u0
+                        a1 = fv * va;           // row v0 + 1, column u0
+                        b0 = (1.0f - fv) * vb;  // row v0, column u0 + 1
+                        b1 = fv * vb;           // row v0 + 1, column u0 + 1
+                    }
+                    const bool in0 = lr >= 0 && lr < kRows, in1 = lr + 1 >= 0 && lr + 1 < kRows;
+                    const int p0 = rpos(lr), p1 = rpos(lr + 1);
+                    if (left && in0) ca_row[p0] += a0;
+                    if (right && in0) cb_row[p0] += b0;
+                    __syncwarp();
+                    if (left && in1) ca_row[p1] += a1;
+                    if (right && in1) cb_row[p1] += b1;
+                    __syncwarp();
                 }
             }
         }
     }
     __syncwarp();
-#pragma unroll
-    for (int k = 0; k < kRPL; ++k) {
-        const int rk = R + lane + k * kFR;
-        if (rk >= g.H) break;
-        float* out = proj + (long long)iv * g.view_stride + (long long)rk * g.W + c;
-        const float acc = srow[lane + k * kFR];
+    // rows R .. R+255 of columns cs0 .. cs0+7: a lane writes one column of a
+    // row, a warp four rows of eight consecutive columns per step
+    for (int idx = lane; idx < kK * kRows; idx += kFR) {
+        const int k = idx % kK, r = idx / kK;
+        const int rk = R + r, ck = cs0 + k;
+        if (rk >= g.H || ck >= g.W) continue;
+        float* out = proj + (long long)iv * g.view_stride + (long long)rk * g.W + ck;
+        const float acc = sacc[k][rpos(r)];
         *out = accumulate ? (*out + acc) : acc;
     }
 }
@@ -196,7 +233,7 @@ int forward_launch(const float* vol, const float4* views, int n_views, const Pro
     int st = layout_launch(vol, g.X, g.Y, g.Zs, CTB_Z_FASTEST, CTB_LITTLE_ENDIAN, volz, s);
     if (st == CTB_OK) {
         dim3 block(kFR, kFC, 1);
-        dim3 grid((g.H + kFR * kRPL - 1) / (kFR * kRPL), (g.W + kFC - 1) / kFC, n_views);
+        dim3 grid((g.H + kRows - 1) / kRows, (g.W + kFC * kK - 1) / (kFC * kK), n_views);
         fp_kernel<<<grid, block, 0, s>>>(volz, views, g, proj, accumulate);
         st = cuda_status(cudaGetLastError(), "fp_kernel launch");
     }

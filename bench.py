@@ -42,10 +42,12 @@ CONFIGS = {
 }
 FILTERS = {"ramlak": 0, "shepplogan": 1, "hann": 2}
 
-# DRAM bytes (read + write) of one backprojection launch per voxel-view update, from one
-# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of a C3 slab launch
-# (1024 x 1024 x 128 voxels x 1440 views of 2048^2, FP16): 173.2 GB / 1.93e11 updates
-BP_DRAM_BYTES_PER_UPDATE = {"c3": (172.619e9 + 0.546e9) / (1024 * 1024 * 128 * 1440)}
+# DRAM bytes (read + write) of one backprojection launch per voxel-view update, from
+# ncu captures (dram__bytes_read.sum + dram__bytes_write.sum) of C3 slab launches
+# (1024 x 1024 x slab voxels x 1440 views of 2048^2, FP16): slab 128: 173.2 GB / 1.93e11
+# updates; slab 512: 938.8 GB / 7.73e11 updates
+BP_DRAM_BYTES_PER_UPDATE = {("c3", 128): (172.619e9 + 0.546e9) / (1024 * 1024 * 128 * 1440),
+                            ("c3", 512): (936.672e9 + 2.172e9) / (1024 * 1024 * 512 * 1440)}
 
 
 # --------------------------------------------------------------------- clocks
@@ -512,7 +514,8 @@ def run_ours(args):
         v.setVolumeBounds(rel[0], rel[1], rel[0], rel[1], rel[0], rel[1])
         v.setFrequencyFilterType(cfg["filter"])
         v.setPrecision(args.store)
-        v.setSlabHeight(slab)
+        if args.e2e_slab > 0:
+            v.setSlabHeight(args.e2e_slab)   # else the facade's own choice (128 slices for 1024^3)
         for _ in range(args.warmup):
             v.reconstructInto(host_out.data_ptr(), L.X_FASTEST)
         barrier(world)
@@ -551,8 +554,8 @@ def run_ours(args):
     filt_gbs = V * H * W * (bytes_px_in + bytes_px_out) / (main["filter_ms"] * 1e-3) / 1e9
     roofline = {"bound": "fetch", "kernel": "bp_tma_kernel", "achieved": bp_gups, "peak": peak_gups, "unit": "GUPS",
                 "frac": bp_gups / peak_gups,
-                "traffic": (BP_DRAM_BYTES_PER_UPDATE[args.config] * X * Y * slab * V
-                            if args.config in BP_DRAM_BYTES_PER_UPDATE and args.store == "fp16" else None),
+                "traffic": (BP_DRAM_BYTES_PER_UPDATE[(args.config, slab)] * X * Y * slab * V
+                            if (args.config, slab) in BP_DRAM_BYTES_PER_UPDATE and args.store == "fp16" else None),
                 "traffic_unit": "DRAM bytes per backprojection launch (one slab)",
                 "algorithmic_bytes_per_launch": 8.0 * X * Y * slab * V,
                 "peak_basis": f"{sm_count} SMs x {clock_mhz:.0f} MHz (median sampled) x 32 lanes / 4 texel loads"}
@@ -655,7 +658,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c3", choices=sorted(CONFIGS))
     ap.add_argument("--store", default="fp16", choices=["fp16", "bf16", "fp32"])
-    ap.add_argument("--slab", type=int, default=128)
+    ap.add_argument("--slab", type=int, default=512, help="z slices per backprojection launch (device-resident leg)")
+    ap.add_argument("--e2e-slab", type=int, default=0, help="slab height of the end-to-end leg (0: the facade's own)")
     ap.add_argument("--subbox", action="store_true", help="reconstruct the 0.25..0.75 sub-box in x, y and z")
     ap.add_argument("--skip-fp32", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")

@@ -735,7 +735,11 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     const size_t view_filt = size_t(pitch) * H * store_bytes(store_);
     const int chunk = int(std::max<size_t>(1, std::min<size_t>(size_t(V), (size_t(256) << 20) / view_raw)));
     const size_t plane = size_t(X) * Y;
-    int slab = slab_req_ > 0 ? slab_req_ : std::max(16, ((Zw + 7) / 8 + 15) / 16 * 16);
+    // default: about a quarter of the slices per slab, a multiple of 16 (C3
+    // end to end: 256 slices 0.6 % faster than 128, fewer launch tails, while
+    // two slabs still cover the upload and the cut last slab keeps the final
+    // download short)
+    int slab = slab_req_ > 0 ? slab_req_ : std::max(16, ((Zw + 3) / 4 + 15) / 16 * 16);
     slab = std::min(slab, Zw);
     const bool convert = order == CTB_Z_FASTEST;
     {

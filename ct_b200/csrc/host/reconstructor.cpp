@@ -735,10 +735,10 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     const size_t view_filt = size_t(pitch) * H * store_bytes(store_);
     const int chunk = int(std::max<size_t>(1, std::min<size_t>(size_t(V), (size_t(256) << 20) / view_raw)));
     const size_t plane = size_t(X) * Y;
-    // default: about a quarter of the slices per slab, a multiple of 16 (C3
-    // end to end: 256 slices 0.6 % faster than 128, fewer launch tails, while
-    // two slabs still cover the upload and the cut last slab keeps the final
-    // download short)
+    // default: about a quarter of the slices per slab, a multiple of 16 (1440
+    // views of 2048^2 into 1024^3, end to end: 256 slices 0.6 % faster than
+    // 128, fewer launch tails, while two slabs still cover the upload and the
+    // cut last slab keeps the final download short)
     int slab = slab_req_ > 0 ? slab_req_ : std::max(16, ((Zw + 3) / 4 + 15) / 16 * 16);
     slab = std::min(slab, Zw);
     const bool convert = order == CTB_Z_FASTEST;
@@ -877,7 +877,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         cudaEventRecord(tf[2 * (c0 / chunk) + 1], w.s_comp);
         cudaEventRecord(ev_free[slot], w.s_comp);
         // the early slabs take the views of every two chunks in one launch
-        // (C3, 32 views per chunk: 1 % faster end to end than every chunk, 4 %
+        // (32 views of 2048^2 per chunk: 1 % faster end to end than every chunk, 4 %
         // slower with four chunks)
         constexpr int kBpGroup = 2;
         if ((c0 / chunk) % kBpGroup == kBpGroup - 1 || c0 + n == V) {

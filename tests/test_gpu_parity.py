@@ -179,7 +179,7 @@ def test_backproject_binned_grid(oracle):
 
 # ---------------------------------------------------------------- end to end
 def c1_scan(tmp_path, n_views=360, W=256, H=192, seed=11):
-    """C1: 360 views over 360 deg, 256x192 at 1.0 mm pitch, SOD 500, SDD 1000, 10 ellipsoids."""
+    """360 views over 360 deg, 256x192 at 1.0 mm pitch, SOD 500, SDD 1000, 10 ellipsoids."""
     geom = synth.ScanGeometry(n_views, W, H, pitch_mm=1.0, sod_mm=500.0, sdd_mm=1000.0)
     scan = synth.make_scan(geom, 10, seed)
     imgs = scan.images.cpu().numpy()
@@ -196,7 +196,7 @@ def test_c1_end_to_end_matches_reference_path(oracle, tmp_path):
     og = oracle.ref_geom(geom.width, geom.height, v.getFCD())
     ref, secs = oracle.ref_reconstruct(imgs, geom.angles(), np.zeros(geom.n_views), 1.0, oracle.RAMLAK, og)
     err = rel_l2(out, ref)
-    print(f"C1 rel-L2 vs reference CPU path: {err:.3e} (CPU {secs:.2f} s)")
+    print(f"360 x 256x192 scan, rel-L2 vs reference CPU path: {err:.3e} (CPU {secs:.2f} s)")
     assert err <= 1e-4
 
 

@@ -71,7 +71,7 @@ def test_window_known_answers(oracle):
 
 
 def test_grid_rule_and_bounds(oracle):
-    # Ct/CtVolume.cpp:311-316, :370-373 with C1 numbers
+    # Ct/CtVolume.cpp:311-316, :370-373 for a 256x192 detector, FCD 1000 px
     assert oracle.cylinder_radius(256, 1000.0) == 126
     g = oracle.ref_geom(256, 192, 1000.0)
     assert (g.xSize, g.ySize, g.zSize) == (252, 252, 192)

@@ -528,7 +528,7 @@ def run_ours(args):
         tm = v.timings()
         sec = max_over_ranks(float(np.mean(ts)), world)
         e2e = {"value": whole_job_gups(units, world, sec * 1e3), "unit": "GUPS", "seconds": sec,
-               "h2d_bytes_per_step": int(V * H * W * 2), "d2h_bytes_per_step": int(X * Y * Z * 4),
+               "h2d_bytes_per_step": int(tm.h2d_bytes), "d2h_bytes_per_step": int(tm.d2h_bytes),
                "stages_s": {"upload_exposed": tm.upload_s, "filter": tm.filter_s, "backproject": tm.backproject_s,
                             "download_exposed": tm.download_s}}
         del v, host_in, host_out

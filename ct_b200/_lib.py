@@ -56,7 +56,8 @@ class Settings(ctypes.Structure):
 
 class Timings(ctypes.Structure):
     _fields_ = [("upload_s", ctypes.c_double), ("filter_s", ctypes.c_double), ("backproject_s", ctypes.c_double),
-                ("download_s", ctypes.c_double), ("total_s", ctypes.c_double), ("voxel_views", ctypes.c_double)]
+                ("download_s", ctypes.c_double), ("total_s", ctypes.c_double), ("voxel_views", ctypes.c_double),
+                ("h2d_bytes", ctypes.c_double), ("d2h_bytes", ctypes.c_double)]
 
 
 PROGRESS_CB = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_double, ctypes.c_void_p)

@@ -660,6 +660,8 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
         t.backproject_s = std::max(t.backproject_s, w->backproject_s);
         t.upload_s = std::max(t.upload_s, w->upload_s);
         t.download_s = std::max(t.download_s, w->download_s);
+        t.h2d_bytes += w->h2d_bytes;
+        t.d2h_bytes += w->d2h_bytes;
     }
     t.total_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     const int step = std::max(1, step_);
@@ -689,6 +691,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         return status;
     };
     w.filter_s = w.backproject_s = w.upload_s = w.download_s = 0;
+    w.h2d_bytes = w.d2h_bytes = 0;
     if (z_hi <= z_lo) return CTB_OK;
     if (cudaSetDevice(w.device) != cudaSuccess) {
         cudaGetLastError();
@@ -727,12 +730,44 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     const float store_scale = store_ == CTB_FP32 ? 1.0f : 1.0f / float(W);
     const float load_scale = store_ == CTB_FP32 ? 1.0f : float(W);
 
+    // ---- detector row band: rows r_lo .. r_lo + Hb - 1 hold every row that
+    // this worker's slices reach (every view, every column of the
+    // reconstruction cylinder, the height offsets, a margin of a few rows).
+    // Only those rows are uploaded, filtered and kept: workers that split z
+    // between devices each move a share of the projections, and a z sub-box
+    // moves only the rows it needs. The rows are filtered independently, so
+    // the band changes no value.
+    int r_lo = 0, Hb = H;
+    {
+        const ProjGeom ga = proj_geom(det_, grid_, z_lo, z_hi, 1.0f);
+        double hlo = 0, hhi = 0;
+        for (int i = 0; i < V; ++i) {
+            hlo = std::min(hlo, hp[i]);
+            hhi = std::max(hhi, hp[i]);
+        }
+        const double R = std::sqrt(double(ga.r2)) + 2.0 * double(ga.vs), D = ga.D;
+        if (R < 0.9 * D) {
+            // row vi = H/2 - (zw + h) U, zw = (j - zPre) vs, U = D / (D - s), |s| <= R
+            const double Umin = D / (D + R), Umax = D / (D - R);
+            const double a = (0.0 - double(ga.zPre)) * ga.vs + hlo, b = (Zw - 1 - double(ga.zPre)) * ga.vs + hhi;
+            const double vmin = std::min(a * Umin, a * Umax), vmax = std::max(b * Umin, b * Umax);
+            const int lo = std::max(0, int(std::floor(double(H) / 2.0 - vmax)) - 3);
+            const int hi = std::min(H - 1, int(std::floor(double(H) / 2.0 - vmin)) + 4);
+            if (hi >= lo) {
+                r_lo = lo;
+                Hb = hi - lo + 1;
+            }
+        }
+    }
+
     // ---- sizing
-    const size_t view_raw = size_t(W) * H * raw_bytes(raw_type_);
+    const size_t row_raw = size_t(W) * raw_bytes(raw_type_);
+    const size_t view_raw_full = row_raw * H;   // one view in the caller's images
+    const size_t view_raw = row_raw * Hb;       // its band on the device
     // filtered rows padded to a 16-byte multiple so every width can use the
     // shared-memory (TMA) backprojector
     const int pitch = (W + 7) / 8 * 8;
-    const size_t view_filt = size_t(pitch) * H * store_bytes(store_);
+    const size_t view_filt = size_t(pitch) * Hb * store_bytes(store_);
     const int chunk = int(std::max<size_t>(1, std::min<size_t>(size_t(V), (size_t(256) << 20) / view_raw)));
     const size_t plane = size_t(X) * Y;
     // default: about a quarter of the slices per slab, a multiple of 16 (1440
@@ -842,7 +877,11 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     auto slab_geom = [&](int zb, int ze) {
         ProjGeom g = proj_geom(det_, grid_, zb, ze, load_scale);
         g.pitch = pitch;
-        g.view_stride = (long long)pitch * H;
+        // rows of the band: row r of the band is detector row r + r_lo
+        g.H = Hb;
+        g.vPre = float(double(H) / 2.0 - double(r_lo));
+        g.vi_hi = float(double(H) - 1 - 0.1 - double(r_lo));
+        g.view_stride = (long long)pitch * Hb;
         return g;
     };
     ProjGeom gpre[2];
@@ -856,13 +895,19 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         const int n = std::min(chunk, V - c0);
         char* dst = (char*)w.d_ring.p + size_t(slot) * view_raw * chunk;
         cudaStreamWaitEvent(w.s_copy, ev_free[slot], 0);
-        if (step_ <= 1) {
+        const char* band0 = (const char*)images_ + size_t(r_lo) * row_raw;
+        if (step_ <= 1 && Hb == H) {
             if (cudaMemcpyAsync(dst, (const char*)images_ + size_t(c0) * view_raw, view_raw * n,
                                 cudaMemcpyHostToDevice, w.s_copy))
                 return cuda_fail("projection upload");
+        } else if (step_ <= 1) {
+            // the band of n consecutive views: n rows of view_raw bytes, view_raw_full apart
+            if (cudaMemcpy2DAsync(dst, view_raw, band0 + size_t(c0) * view_raw_full, view_raw_full, view_raw, n,
+                                  cudaMemcpyHostToDevice, w.s_copy))
+                return cuda_fail("projection upload");
         } else {
             for (int i = 0; i < n; ++i)
-                if (cudaMemcpyAsync(dst + size_t(i) * view_raw, (const char*)images_ + size_t(used[c0 + i]) * view_raw,
+                if (cudaMemcpyAsync(dst + size_t(i) * view_raw, band0 + size_t(used[c0 + i]) * view_raw_full,
                                     view_raw, cudaMemcpyHostToDevice, w.s_copy))
                     return cuda_fail("projection upload");
         }
@@ -870,6 +915,8 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
         cudaStreamWaitEvent(w.s_comp, ev_up[slot], 0);
         FilterArgs fa = filter_args(det_, raw_type_, M, logM, n, store_scale);
         fa.out_pitch = pitch;
+        fa.H = Hb;                                         // the band's rows,
+        fa.vPre = float(double(H) / 2.0 - double(r_lo));  // weighted as detector rows r + r_lo
         cudaEventRecord(tf[2 * (c0 / chunk)], w.s_comp);
         char* fdst = (char*)w.d_filtered.p + size_t(c0) * view_filt;
         if (filter_launch(dst, raw_type_, fdst, store_, fa, (const float2*)w.d_tw.p, (const float*)w.d_K.p, w.s_comp))
@@ -990,6 +1037,8 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     w.backproject_s = b_ms * 1e-3;
     w.upload_s = std::max(0.0, (phase_ms - f_ms - bp0_ms) * 1e-3);
     w.download_s = std::max(0.0, total - (phase_ms + tail_ms) * 1e-3);
+    w.h2d_bytes = double(view_raw) * V;
+    w.d2h_bytes = double(plane) * Zw * sizeof(float);
     return CTB_OK;
 }
 

@@ -49,6 +49,7 @@ struct DeviceWork {
     // outcome of the last run
     std::string err;
     double filter_s = 0, backproject_s = 0, upload_s = 0, download_s = 0;
+    double h2d_bytes = 0, d2h_bytes = 0;
     double progress = 0;  // 0..1 of this worker's slices
     double share = 1;     // this worker's fraction of all slices
     explicit DeviceWork(int d) : device(d) {}

@@ -303,6 +303,9 @@ typedef struct {
     double download_s;      /* device->host copies not hidden behind backprojection */
     double total_s;         /* wall time of the whole call */
     double voxel_views;     /* x*y*z*views processed */
+    double h2d_bytes;       /* projection bytes copied host->device (each device
+                               copies only the detector rows its slices reach) */
+    double d2h_bytes;       /* volume bytes copied device->host */
 } ctb_timings;
 int ctb_get_timings(const ctb_ctx* ctx, ctb_timings* t);
 

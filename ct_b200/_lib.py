@@ -71,6 +71,7 @@ SIGNATURES = {
     "ctb_device_name": (I, [I, ctypes.c_char_p, Z]),
     "ctb_free_memory": (I, [I, P, P]),
     "ctb_reference_grid": (I, [P, P, P]),
+    "ctb_row_band": (I, [P, P, I, I, P, I, P, P]),
     "ctb_filter_projections": (I, [P, I, I, P, I, I, P, I, F, P]),
     "ctb_backproject": (I, [P, I, I, P, P, P, P, I, I, F, P, I, P]),
     "ctb_backproject_noalloc": (I, [P, I, I, P, P, P, P, I, I, F, P, I, P]),

@@ -108,6 +108,16 @@ int ctb_reference_grid(ctb_detector* det, const float rel6[6], ctb_grid* grid) {
     return CTB_OK;
 }
 
+int ctb_row_band(const ctb_detector* det, const ctb_grid* grid, int z_begin, int z_end,
+                 const double* height_offsets_px, int n_views, int* r_lo, int* rows) {
+    if (!det || !grid || !r_lo || !rows || !valid_detector(det) || !valid_grid(grid) || n_views < 0)
+        return arg_error("invalid row band arguments");
+    if (det->radius <= 0) return arg_error("detector radius not set (use ctb_reference_grid)");
+    if (z_begin < 0 || z_end <= z_begin || z_end > grid->z_to - grid->z_from) return arg_error("invalid z range");
+    ctb::row_band(*det, *grid, z_begin, z_end, height_offsets_px, n_views, r_lo, rows);
+    return CTB_OK;
+}
+
 int ctb_filter_projections(const void* raw, int raw_type, int n_views, const ctb_detector* det, int filter,
                            int pad, void* filtered, int store_type, float store_scale, void* stream) {
     if (!raw || !filtered || n_views < 0 || !valid_detector(det)) return arg_error("invalid filter arguments");

@@ -113,6 +113,14 @@ struct ProjGeom {
 
 ProjGeom proj_geom(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_end, float load_scale);
 
+// The band of detector rows r_lo .. r_lo + rows - 1 that the voxels of box
+// slices [z_begin, z_end) reach in any view with the given height offsets
+// (pixels), every column of the reconstruction cylinder, with their bilinear
+// neighbours and a margin of a few rows; the whole detector when no tighter
+// bound applies.
+void row_band(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_end, const double* heights_px,
+              int n_views, int* r_lo, int* rows);
+
 // Backprojection of views [0, n) from `views` (device view table) into vol.
 // hmax bounds |height offset| (pixels) over the views. Dispatches to the
 // shared-memory (TMA) kernel when possible, else to the global-gather kernel.

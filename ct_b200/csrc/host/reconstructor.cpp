@@ -684,6 +684,33 @@ void Reconstructor::worker_progress(DeviceWork& w, double frac, const float* pre
 // Reconstructs box slices [z_lo, z_hi) on worker w's device into out, which
 // holds the whole box in the requested index order (cudaReconstructionCore,
 // Ct/CtVolume.cpp:1155-1320, for one device's part of the volume).
+void row_band(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_end, const double* heights_px,
+              int n_views, int* r_lo, int* rows) {
+    const int H = det.height;
+    *r_lo = 0;
+    *rows = H;
+    if (z_end <= z_begin) return;
+    const ProjGeom ga = proj_geom(det, grid, z_begin, z_end, 1.0f);
+    double hlo = 0, hhi = 0;
+    for (int i = 0; i < n_views && heights_px; ++i) {
+        hlo = std::min(hlo, heights_px[i]);
+        hhi = std::max(hhi, heights_px[i]);
+    }
+    const double R = std::sqrt(double(ga.r2)) + 2.0 * double(ga.vs), D = ga.D;
+    if (!(R < 0.9 * D)) return;
+    // row vi = H/2 - (zw + h) U with zw = (j - zPre) vs, U = D / (D - s), |s| <= R
+    const double Umin = D / (D + R), Umax = D / (D - R);
+    const double a = (0.0 - double(ga.zPre)) * ga.vs + hlo;
+    const double b = (double(z_end - z_begin) - 1.0 - double(ga.zPre)) * ga.vs + hhi;
+    const double vmin = std::min(a * Umin, a * Umax), vmax = std::max(b * Umin, b * Umax);
+    const int lo = std::max(0, int(std::floor(std::max(-1.0e9, double(H) / 2.0 - vmax))) - 3);
+    const int hi = std::min(H - 1, int(std::floor(std::min(1.0e9, double(H) / 2.0 - vmin))) + 4);
+    if (hi >= lo) {
+        *r_lo = lo;
+        *rows = hi - lo + 1;
+    }
+}
+
 int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, int z_hi) {
     const auto t_start = std::chrono::steady_clock::now();
     auto fail = [&w](int status, const std::string& msg) {
@@ -738,27 +765,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     // moves only the rows it needs. The rows are filtered independently, so
     // the band changes no value.
     int r_lo = 0, Hb = H;
-    {
-        const ProjGeom ga = proj_geom(det_, grid_, z_lo, z_hi, 1.0f);
-        double hlo = 0, hhi = 0;
-        for (int i = 0; i < V; ++i) {
-            hlo = std::min(hlo, hp[i]);
-            hhi = std::max(hhi, hp[i]);
-        }
-        const double R = std::sqrt(double(ga.r2)) + 2.0 * double(ga.vs), D = ga.D;
-        if (R < 0.9 * D) {
-            // row vi = H/2 - (zw + h) U, zw = (j - zPre) vs, U = D / (D - s), |s| <= R
-            const double Umin = D / (D + R), Umax = D / (D - R);
-            const double a = (0.0 - double(ga.zPre)) * ga.vs + hlo, b = (Zw - 1 - double(ga.zPre)) * ga.vs + hhi;
-            const double vmin = std::min(a * Umin, a * Umax), vmax = std::max(b * Umin, b * Umax);
-            const int lo = std::max(0, int(std::floor(double(H) / 2.0 - vmax)) - 3);
-            const int hi = std::min(H - 1, int(std::floor(double(H) / 2.0 - vmin)) + 4);
-            if (hi >= lo) {
-                r_lo = lo;
-                Hb = hi - lo + 1;
-            }
-        }
-    }
+    row_band(det_, grid_, z_lo, z_hi, hp.data(), V, &r_lo, &Hb);
 
     // ---- sizing
     const size_t row_raw = size_t(W) * raw_bytes(raw_type_);

@@ -41,6 +41,16 @@ def detector(width, height, fcd, u_offset=0.0, base_intensity=1.0, rel=None):
     return d, g
 
 
+def row_band(d: L.Detector, g: L.Grid, z_begin: int, z_end: int, heights_px=None):
+    """Detector rows (r_lo, rows) that box slices [z_begin, z_end) reach (host only)."""
+    h = None if heights_px is None else np.ascontiguousarray(heights_px, dtype=np.float64)
+    n = 0 if h is None else len(h)
+    r_lo, rows = ctypes.c_int(), ctypes.c_int()
+    check(lib().ctb_row_band(ctypes.byref(d), ctypes.byref(g), int(z_begin), int(z_end),
+                             None if h is None else h.ctypes.data, n, ctypes.byref(r_lo), ctypes.byref(rows)))
+    return r_lo.value, rows.value
+
+
 def custom_grid(d: L.Detector, size, voxel_pitch, box=None) -> L.Grid:
     x, y, z = size
     if box is None:

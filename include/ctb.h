@@ -98,6 +98,15 @@ int ctb_free_memory(int device, size_t* free_bytes, size_t* total_bytes);
  * zmin,zmax} clamped like setVolumeBounds (:487-500). det->radius is set. */
 int ctb_reference_grid(ctb_detector* det, const float rel6[6], ctb_grid* grid);
 
+/* Detector rows [*r_lo, *r_lo + *rows) that the voxels of box slices
+ * [z_begin, z_end) reach in any of n views with the given height offsets
+ * (pixels; NULL = none), bilinear neighbours and a margin included: the rows a
+ * device reconstructing only those slices needs to upload and filter (the
+ * facade does so per device). No reference counterpart: the reference
+ * uploads and filters every row on every device. det->radius must be set. */
+int ctb_row_band(const ctb_detector* det, const ctb_grid* grid, int z_begin, int z_end,
+                 const double* height_offsets_px, int n_views, int* r_lo, int* rows);
+
 /* Preprocess and ramp-filter n_views raw projections in one launch sequence:
  * -ln of the normalised intensity, Feldkamp cosine weight, and the row-wise
  * ramp filter (ramlak / shepplogan / hann) applied in frequency with the

@@ -266,3 +266,69 @@ def test_remaining_facade_getters_and_setters(tmp_path):
     X, Y, Z = v.getXSize(), v.getYSize(), v.getZSize()
     assert v.getRequiredMemoryUpperBound() == X * Y * Z * 4 + 12 * 8 * 4 * 1 * 3
     assert isinstance(CtVolume.cudaAvailable(), bool)
+
+
+def _rows_reached(det, grid, z0, z1, heights, rng, n_cols=6000, n_ang=180):
+    """Brute force in float64: the detector rows (v0 and v0 + 1 of the bilinear
+    sample) of voxels in the cylinder, inside the u and v bounds
+    (Ct/CtVolume.cpp:923-1011), for box slices z0 and z1 - 1 (the row is
+    monotone in z), over random columns and angles."""
+    W, H, D, uoff, r2 = det.width, det.height, det.fcd, det.u_offset, det.radius ** 2
+    vs = grid.voxel_pitch
+    xpre = grid.x_size / 2 - grid.x_from
+    ypre = grid.y_size / 2 - grid.y_from
+    zpre = grid.z_size / 2 - grid.z_from
+    X, Y = grid.x_to - grid.x_from, grid.y_to - grid.y_from
+    ix = rng.integers(0, X, n_cols)
+    iy = rng.integers(0, Y, n_cols)
+    # the cylinder's rim, where the magnification is largest
+    phi = rng.uniform(0, 2 * np.pi, n_cols)
+    rim = np.sqrt(r2) * 0.999
+    ix = np.concatenate([ix, np.clip(np.round(rim * np.cos(phi) / vs + xpre), 0, X - 1)]).astype(int)
+    iy = np.concatenate([iy, np.clip(np.round(rim * np.sin(phi) / vs + ypre), 0, Y - 1)]).astype(int)
+    x, y = (ix - xpre) * vs, (iy - ypre) * vs
+    keep = x * x + y * y < r2
+    x, y = x[keep], y[keep]
+    rows = []
+    hs = np.zeros(1) if heights is None else np.asarray(heights)
+    for th in rng.uniform(0, 2 * np.pi, n_ang):
+        sn, cs = np.sin(th), np.cos(th)
+        s = x * cs + y * sn
+        t = -x * sn + y * cs + uoff
+        U = D / (D - s)
+        u = t * U
+        ok = (u >= -W / 2) & (u <= W - 1.1 - W / 2)
+        for zi in (z0, z1 - 1):
+            zw = (zi - zpre) * vs
+            for h in hs:
+                v = (zw + h) * U[ok]
+                vok = (v >= -(H - 1 - 0.1) + H / 2) & (v <= H / 2)
+                vi = -v[vok] + H / 2
+                r = np.floor(vi).astype(int)
+                rows.append(r)
+                rows.append(r + 1)
+    return np.concatenate(rows) if rows else np.zeros(0, int)
+
+
+def test_row_band_covers_every_row_reached():
+    from ct_b200 import ops
+    rng = np.random.default_rng(11)
+    shrunk = 0
+    for k in range(24):
+        W, H = int(rng.integers(24, 400)), int(rng.integers(16, 400))
+        fcd = float(rng.uniform(1.5 * W, 10 * W))
+        det, grid = ops.detector(W, H, fcd, u_offset=float(rng.choice([0.0, 2.5, -4.0])))
+        Z = grid.z_to - grid.z_from
+        z0 = int(rng.integers(0, Z))
+        z1 = int(rng.integers(z0 + 1, Z + 1))
+        heights = rng.uniform(-4, 4, 16) if k % 2 else None
+        r_lo, n = ops.row_band(det, grid, z0, z1, heights)
+        assert 0 <= r_lo and n >= 1 and r_lo + n <= H
+        r = _rows_reached(det, grid, z0, z1, heights, rng)
+        if r.size:
+            assert r.min() >= r_lo and r.max() <= r_lo + n - 1, (k, r.min(), r.max(), r_lo, n)
+        shrunk += n < H
+    assert shrunk >= 8   # thin slabs really do get a narrower band
+    # the whole box reaches the whole detector (rows clipped to it)
+    det, grid = ops.detector(256, 192, 1000.0)
+    assert ops.row_band(det, grid, 0, grid.z_to - grid.z_from) == (0, 192)

@@ -762,8 +762,9 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     // reconstruction cylinder, the height offsets, a margin of a few rows).
     // Only those rows are uploaded, filtered and kept: workers that split z
     // between devices each move a share of the projections, and a z sub-box
-    // moves only the rows it needs. The rows are filtered independently, so
-    // the band changes no value.
+    // moves only the rows it needs. Rows are filtered independently, so the
+    // filtered values do not change; the backprojector's row coordinates are
+    // rounded from the band's first row (differences of a few ulps).
     int r_lo = 0, Hb = H;
     row_band(det_, grid_, z_lo, z_hi, hp.data(), V, &r_lo, &Hb);
 

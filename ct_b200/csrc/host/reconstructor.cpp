@@ -2,13 +2,15 @@
 //
 // Pipeline of one reconstruction on one B200 (all views' filtered projections
 // stay resident in HBM; the volume streams out in z-slabs):
-//   copy stream    : H2D of raw u8/u16/f32 projections in chunks of views,
-//                    into a 3-slot ring of device buffers
+//   copy stream    : H2D of the detector rows this device's slices reach, in
+//                    chunks of views, into a 3-slot ring of device buffers
 //   compute stream : fused preprocess + ramp filter of each chunk (kernel a+b)
-//                    into the resident filtered set (FP32/FP16/BF16), then
-//                    one backprojection launch per z-slab over all views
-//                    (kernel c), then the output layout kernel
+//                    into the resident filtered set (FP32/FP16/BF16); the
+//                    first two slabs are backprojected every two chunks while
+//                    the views arrive, every later slab in one launch over all
+//                    views (kernel c); then the output layout kernel
 //   download stream: D2H of each finished slab while the next slab computes
+//                    (three slab buffers; a short last slab)
 // The reference instead re-reads and re-filters every projection for every
 // VRAM-sized chunk and launches one kernel per view (Ct/CtVolume.cpp:1155-1301).
 

@@ -21,12 +21,16 @@ struct Image {
     std::vector<uint8_t> data;  // row-major, native-endian samples
 };
 
-// Reads only the header: size and sample type. Returns false with a message.
+// The size and sample type from the header. Returns false with a message.
 bool probe_image(const std::string& path, int* width, int* height, int* type, std::string* err);
 
 // Decodes the image into dst (width*height samples of `type`), which must be
 // large enough. Returns false with a message on failure.
 bool decode_image_into(const std::string& path, int width, int height, int type, void* dst, std::string* err);
+// Both in one read of the file: the image's size and depth must be the given
+// ones (the projections of one scan), then its samples go to dst.
+enum { kLoadOk = 0, kLoadUnreadable = 1, kLoadOtherSize = 2, kLoadOtherDepth = 3 };
+int load_image_into(const std::string& path, int width, int height, int type, void* dst, std::string* err);
 
 bool decode_image(const std::string& path, Image* img, std::string* err);
 

@@ -494,13 +494,11 @@ int Reconstructor::load_csv(const std::string& csv_path) {
     std::atomic<size_t> done{0};
     parallel_for(paths.size(), [&](size_t i) {
         if (bad.load() >= 0 || stop_) return;
-        int w = 0, hh = 0, t = 0;
         std::string er;
-        bool good = probe_image(paths[i], &w, &hh, &t, &er);
-        if (good && (w != W || hh != H)) { good = false; er = "dims"; }
-        if (good && t != type) { good = false; er = "depth"; }
-        if (good) good = decode_image_into(paths[i], W, H, type, (char*)images_owned_.p + i * bytes_per, &er);
-        if (!good) {
+        const int r = load_image_into(paths[i], W, H, type, (char*)images_owned_.p + i * bytes_per, &er);
+        if (r == kLoadOtherSize) er = "dims";
+        if (r == kLoadOtherDepth) er = "depth";
+        if (r != kLoadOk) {
             errs[i] = er;
             int expect = -1;
             bad.compare_exchange_strong(expect, int(i));

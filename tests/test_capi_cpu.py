@@ -332,3 +332,31 @@ def test_row_band_covers_every_row_reached():
     # the whole box reaches the whole detector (rows clipped to it)
     det, grid = ops.detector(256, 192, 1000.0)
     assert ops.row_band(det, grid, 0, grid.z_to - grid.z_from) == (0, 192)
+
+
+@pytest.mark.parametrize("pattern", ["constant", "ramp", "repeat", "noise", "sparse"])
+def test_lzw_tiff_patterns_match_cv2(tmp_path, pattern):
+    """LZW strings of every kind: runs that hit the code being defined (constant and
+    repeating rows), full tables that force clear codes (noise over 1024^2), code widths
+    9 to 12, and strips whose last code ends the strip exactly."""
+    cv2 = pytest.importorskip("cv2")
+    from ct_b200.ctvolume import read_image
+    rng = np.random.default_rng(3)
+    H, W = 1024, 1024
+    if pattern == "constant":
+        img = np.full((H, W), 4321, np.uint16)
+    elif pattern == "ramp":
+        img = (np.arange(H * W, dtype=np.uint32) % 65536).astype(np.uint16).reshape(H, W)
+    elif pattern == "repeat":
+        img = np.tile(rng.integers(0, 65536, 37, dtype=np.uint16), H * W // 37 + 1)[:H * W].reshape(H, W)
+    elif pattern == "noise":
+        img = rng.integers(0, 65536, (H, W), dtype=np.uint16)
+    else:
+        img = np.zeros((H, W), np.uint16)
+        img[rng.integers(0, H, 500), rng.integers(0, W, 500)] = rng.integers(1, 65536, 500)
+    for depth_img in (img, (img >> 8).astype(np.uint8)):
+        path = str(tmp_path / f"{pattern}_{depth_img.dtype}.tif")
+        assert cv2.imwrite(path, depth_img, [cv2.IMWRITE_TIFF_COMPRESSION, 5])
+        ref = cv2.imread(path, cv2.IMREAD_GRAYSCALE | cv2.IMREAD_ANYDEPTH)
+        got = read_image(path)
+        assert got.dtype == ref.dtype and np.array_equal(got, ref), (pattern, depth_img.dtype)

@@ -401,7 +401,9 @@ void orc_ref_fix_sinogram(double* angles, double* heights, int n, int ccw, doubl
     double sum = 0;
     for (int i = 0; i < n; ++i) sum += heights[i];
     sum /= double(n);
-    for (int i = 0; i < n; ++i) { heights[i] -= sum; heights[i] /= pixelSize; }
+    // pixelSize is a float member of the reference's CtVolume (Ct/CtVolume.h:224)
+    const double pix = double(float(pixelSize));
+    for (int i = 0; i < n; ++i) { heights[i] -= sum; heights[i] /= pix; }
 }
 
 // The reference's window value for bin k of nyq bins.

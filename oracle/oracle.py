@@ -236,3 +236,102 @@ def rel_err(x: np.ndarray, ref: np.ndarray) -> RelErr:
     d = x - ref
     n = np.linalg.norm(ref.ravel())
     return RelErr(float(np.linalg.norm(d.ravel()) / (n if n > 0 else 1.0)), float(np.abs(d).max(initial=0.0)))
+
+
+# --------------------------------------------- the reference's own CPU code
+# oracle/_ref/libct_ref.so: the reference's CPU reconstruction lines of
+# Ct/CtVolume.cpp compiled unchanged (oracle/Makefile target `ref`, shims in
+# oracle/ref_shim.h, driver in oracle/ref_build.cpp). Built where the
+# reference sources are present; the built library travels with the tree.
+_REF_LIB_PATH = os.path.join(_HERE, "_ref", "libct_ref.so")
+# the same lines built with <cmath> alone (libstdc++): sqrt/sin/cos of a float
+# resolve to the double functions there
+_REF_GCC_LIB_PATH = os.path.join(_HERE, "_ref", "libct_ref_gcc.so")
+_REF_SOURCE = "/root/reference/Ct/CtVolume.cpp"
+_ref_libs = {}
+
+
+def build_ref() -> str | None:
+    """Build oracle/_ref/libct_ref.so from the reference sources if they are
+    present; returns the library path, or None when neither exists."""
+    if os.path.exists(_REF_SOURCE):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    return _REF_LIB_PATH if os.path.exists(_REF_LIB_PATH) else None
+
+
+def ref_source_available() -> bool:
+    return os.path.exists(_REF_LIB_PATH) or os.path.exists(_REF_SOURCE)
+
+
+def ref_lib(variant: str = "msvc"):
+    """variant "msvc": float overloads of sqrt/sin/cos in the global namespace
+    (the reference's Windows build); "gcc": <cmath> alone under libstdc++."""
+    if variant not in _ref_libs:
+        if build_ref() is None:
+            raise FileNotFoundError("oracle/_ref/libct_ref.so is not built and the reference sources are absent")
+        L = ctypes.CDLL(_REF_LIB_PATH if variant == "msvc" else _REF_GCC_LIB_PATH)
+        P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        L.ref_reconstruct.restype = I
+        L.ref_reconstruct.argtypes = [P, I, I, I, I, P, P, D, D, D, D, ctypes.c_char_p, P, I, ctypes.c_uint, P, P,
+                                      P]
+        L.ref_prepare_projection.restype = I
+        L.ref_prepare_projection.argtypes = [P, I, I, I, I, P, D, D, D, I, I, P]
+        L.ref_fix_sinogram.restype = I
+        L.ref_fix_sinogram.argtypes = [I, P, P, D, ctypes.c_char_p, P, P]
+        _ref_libs[variant] = L
+    return _ref_libs[variant]
+
+
+def refsrc_reconstruct(imgs: np.ndarray, angles_deg, heights_mm, pixel_size: float, fcd_mm: float,
+                       u_offset_mm: float = 0.0, base: float = 1.0, rotation: str = "ccw", rel=None,
+                       filter_type: int = RAMLAK, skip: int = 0, dims_only: bool = False,
+                       variant: str = "msvc"):
+    """The reference's own CPU reconstruction (CSV values as they appear in the
+    file: angles in degrees, heights and distances in mm). Returns
+    (volume (x, y, z) Z_FASTEST, seconds of reconstructionCore), or the box
+    dimensions with dims_only."""
+    imgs = np.ascontiguousarray(imgs)
+    V, H, W = imgs.shape
+    a = np.ascontiguousarray(angles_deg, np.float64)
+    h = None if heights_mm is None else np.ascontiguousarray(heights_mm, np.float64)
+    r6 = None if rel is None else np.ascontiguousarray(rel, np.float32)
+    dims = np.zeros(3, np.int32)
+    L = ref_lib(variant)
+    args = (_p(imgs), _depth(imgs[0]), V, W, H, _p(a), None if h is None else _p(h), pixel_size, u_offset_mm,
+            fcd_mm, base, rotation.encode(), None if r6 is None else _p(r6), filter_type, skip)
+    st = L.ref_reconstruct(*args, None, _p(dims), None)
+    if st != 0:
+        raise RuntimeError(f"ref_reconstruct failed ({st})")
+    if dims_only:
+        return tuple(int(d) for d in dims)
+    vol = np.zeros(tuple(int(d) for d in dims), np.float32)
+    secs = ctypes.c_double(0)
+    st = L.ref_reconstruct(*args, _p(vol), _p(dims), ctypes.byref(secs))
+    if st != 0:
+        raise RuntimeError(f"ref_reconstruct failed ({st})")
+    return vol, secs.value
+
+
+def refsrc_prepare_projection(imgs: np.ndarray, index: int, pixel_size: float, fcd_mm: float, base: float = 1.0,
+                              filter_type: int = RAMLAK, variant: str = "msvc") -> np.ndarray:
+    """The reference's prepareProjection of view `index` (H x W float32)."""
+    imgs = np.ascontiguousarray(imgs)
+    V, H, W = imgs.shape
+    a = np.zeros(V, np.float64)
+    out = np.empty((H, W), np.float32)
+    st = ref_lib(variant).ref_prepare_projection(_p(imgs), _depth(imgs[0]), V, W, H, _p(a), pixel_size, fcd_mm, base,
+                                          filter_type, index, _p(out))
+    if st != 0:
+        raise RuntimeError(f"ref_prepare_projection failed ({st})")
+    return out
+
+
+def refsrc_fix_sinogram(angles_deg, heights_mm, pixel_size: float, rotation: str):
+    """The reference's makeHeightOffsetRelative + correctAngleDirection:
+    (angles in degrees, relative height offsets in pixels)."""
+    a = np.ascontiguousarray(angles_deg, np.float64)
+    h = np.ascontiguousarray(heights_mm, np.float64)
+    ao = np.empty_like(a)
+    ho = np.empty_like(a)
+    ref_lib().ref_fix_sinogram(len(a), _p(a), _p(h), pixel_size, rotation.encode(), _p(ao), _p(ho))
+    return ao, ho

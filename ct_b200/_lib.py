@@ -76,6 +76,7 @@ SIGNATURES = {
     "ctb_backproject": (I, [P, I, I, P, P, P, P, I, I, F, P, I, P]),
     "ctb_backproject_noalloc": (I, [P, I, I, P, P, P, P, I, I, F, P, I, P]),
     "ctb_forward_project": (I, [P, P, P, I, P, P, I, I, P, I, P]),
+    "ctb_diag_force_overflow": (None, [I]),
     "ctb_convert_layout": (I, [P, I, I, I, I, I, P, P]),
     "ctb_create": (I, [P]),
     "ctb_destroy": (None, [P]),

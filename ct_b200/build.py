@@ -89,7 +89,7 @@ def build(verbose: bool = False, clean: bool = False) -> str:
         subprocess.run(cmd, check=True)
     cli_src = os.path.join(CSRC, "cli.cpp")
     if os.path.exists(cli_src) and _newer(CLI, [cli_src, LIB, os.path.join(ROOT, "include", "ctb.h")]):
-        cmd = [NVCC] + COMMON + ["-o", CLI, cli_src, f"-L{HERE}", "-lctb", "-Xlinker", "-rpath,$ORIGIN"]
+        cmd = [NVCC] + ARCH + COMMON + ["-o", CLI, cli_src, f"-L{HERE}", "-lctb", "-Xlinker", "-rpath,$ORIGIN"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

@@ -19,14 +19,8 @@ struct ctb_ctx {
 
 namespace {
 
-bool valid_detector(const ctb_detector* d) {
-    return d && d->width > 1 && d->height > 1 && d->fcd > float(d->width) && d->base_intensity != 0.0f;
-}
-
-bool valid_grid(const ctb_grid* g) {
-    return g && g->x_size > 0 && g->y_size > 0 && g->z_size > 0 && g->x_from >= 0 && g->x_to > g->x_from &&
-           g->y_from >= 0 && g->y_to > g->y_from && g->z_from >= 0 && g->z_to > g->z_from && g->voxel_pitch > 0;
-}
+using ctb::valid_detector;
+using ctb::valid_grid;
 
 int arg_error(const char* msg) {
     ctb::set_global_error(msg);
@@ -184,6 +178,8 @@ int ctb_diag_bounded_wait(int device, unsigned limit) {
     cudaSetDevice(prev);
     return st;
 }
+
+void ctb_diag_force_overflow(int every) { ctb::bp_force_overflow(every); }
 
 int ctb_forward_project(const float* vol, const double* angles_deg, const double* height_offsets_px, int n_views,
                         const ctb_detector* det, const ctb_grid* grid, int z_begin, int z_end, float* proj,

@@ -31,6 +31,15 @@ int cuda_status(cudaError_t e, const char* what);
 // invalidated by another thread lowering it.
 int ensure_dynamic_smem(const void* kernel, size_t bytes);
 
+// Argument checks shared by the operator entry points.
+inline bool valid_detector(const ctb_detector* d) {
+    return d && d->width > 1 && d->height > 1 && d->fcd > float(d->width) && d->base_intensity != 0.0f;
+}
+inline bool valid_grid(const ctb_grid* g) {
+    return g && g->x_size > 0 && g->y_size > 0 && g->z_size > 0 && g->x_from >= 0 && g->x_to > g->x_from &&
+           g->y_from >= 0 && g->y_to > g->y_from && g->z_from >= 0 && g->z_to > g->z_from && g->voxel_pitch > 0;
+}
+
 inline size_t store_bytes(int store_type) { return store_type == CTB_FP32 ? 4 : 2; }
 inline size_t raw_bytes(int raw_type) { return raw_type == CTB_U8 ? 1 : raw_type == CTB_U16 ? 2 : 4; }
 
@@ -162,6 +171,10 @@ int bp_batch_plan(int store_type, int zc, const BpBatchScan* scans, int n, BpBat
 // device counter that must be zero at launch.
 int bp_batch_launch(const BpBatchPlan& plan, const void* desc, const long long* tile_start, int n,
                     unsigned long long* queue, cudaStream_t s);
+// Diagnostic: from the next launch on, views whose index is a multiple of
+// `every` read their texels through global memory, as views whose footprint
+// exceeds the box do (0 = off). Results do not change.
+void bp_force_overflow(int every);
 // Number of CTAs whose bounded mbarrier waits gave up since the last reset.
 int device_wait_timeouts(unsigned* count, int reset);
 // Run a wait that can never complete with the given try limit (diagnostic of

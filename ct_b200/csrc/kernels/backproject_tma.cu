@@ -25,6 +25,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -37,6 +38,9 @@ namespace ctb {
 __device__ unsigned int g_wait_timeouts = 0;
 
 namespace {
+
+// diagnostic: every k-th view reads through global memory (0 = off)
+std::atomic<int> g_ovf_every{0};
 
 constexpr int kTX = 32, kTY = 8;
 constexpr unsigned kWaitLimit = 1u << 26;
@@ -124,6 +128,8 @@ struct Box {
     int BU, BV;          // box columns / rows (elements)
     int buf_elems;       // elements per buffer (BU * BV rounded to 128 bytes)
     float vi_hi;         // upper bound of the row coordinate: float(H - 1.1)
+    int ovf_every;       // diagnostic: views whose index is a multiple of this
+                         // take the global-memory path as if they overflowed (0 = off)
 };
 
 // 8 consumer warps own the tile's columns; warp 8 is the producer that waits
@@ -141,6 +147,7 @@ struct Pipe {
     uint64_t empty[NBUF];   // every consumer warp finished reading the box
     int2 org[NBUF];         // box origin (column, row)
     float4 qv[NBUF];        // {sin, cos, h} of the view in each buffer
+    int vv[NBUF];           // index of the view in each buffer
     int ovf[NBUF];          // footprint larger than the box: read global memory
     int abort_flag;         // a bounded wait gave up
     long long item;         // persistent kernel: current work item
@@ -256,7 +263,9 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                 const int vo = int(floorf(vmin)) - 2;
                 p.org[b] = make_int2(uo, vo);
                 p.qv[b] = q;
-                p.ovf[b] = (int(floorf(umax)) + 3 - uo > bx.BU) || (int(floorf(vmax)) + 3 - vo > bx.BV);
+                p.vv[b] = vv;
+                p.ovf[b] = (int(floorf(umax)) + 3 - uo > bx.BU) || (int(floorf(vmax)) + 3 - vo > bx.BV) ||
+                           (bx.ovf_every > 0 && vv % bx.ovf_every == 0);
                 mbar_expect_tx(&p.full[b], uint32_t(bx.BU) * bx.BV * sizeof(T));
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 tma_load_3d(buf + size_t(b) * buf_stride, map, uo, vo, vv, &p.full[b]);
@@ -322,7 +331,8 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                         }
                     }
                 } else {
-                    const T* col = proj + (long long)iv * g.view_stride + u0;
+                    // the view staged in this buffer (the tile's view order is rotated)
+                    const T* col = proj + (long long)p.vv[b] * g.view_stride + u0;
                     int ja, jb;
                     v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);
 #pragma unroll
@@ -525,6 +535,7 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     b->BV = BV;
     b->buf_elems = (BU * BV + per128 - 1) / per128 * per128;
     b->vi_hi = float(double(g.H) - 1 - 0.1);
+    b->ovf_every = g_ovf_every.load();
     return true;
 }
 
@@ -746,6 +757,8 @@ int bounded_wait_probe_run(unsigned limit, cudaStream_t s) {
     }
     return CTB_OK;
 }
+
+void bp_force_overflow(int every) { g_ovf_every.store(every > 0 ? every : 0); }
 
 int device_wait_timeouts(unsigned* count, int reset) {
     CTB_CUDA_TRY(cudaMemcpyFromSymbol(count, g_wait_timeouts, sizeof(unsigned)));

@@ -143,9 +143,13 @@ int ctb_backproject(const void* filtered, int store_type, int n_views, const dou
  * at every call lives in a static 256 KB device array of the library instead,
  * so this call allocates nothing (the caller passes the filtered projections
  * and the volume, as before). At most CTB_NOALLOC_MAX_VIEWS views per call
- * (CTB_ERR_UNSUPPORTED beyond that). The first call on a device looks up the
- * array's address; make it before any stream capture. All calls share the
- * array: calls that overlap on the GPU race, so serialise them. */
+ * (CTB_ERR_UNSUPPORTED beyond that); larger sets of views are split into
+ * several calls with accumulate = 1. Arguments are checked as ctb_backproject
+ * checks them. The first call on a device looks up the array's address, which
+ * with lazy module loading also loads the library's kernels onto the device
+ * (device memory taken once): make it at start-up, before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race, so serialise
+ * them. */
 #define CTB_NOALLOC_MAX_VIEWS 8192
 int ctb_backproject_noalloc(const void* filtered, int store_type, int n_views, const double* angles_deg,
                             const double* height_offsets_px, const ctb_detector* det, const ctb_grid* grid,
@@ -358,6 +362,13 @@ int ctb_device_wait_timeouts(int device, unsigned* count, int reset);
  * complete, with at most `limit` tries, and must give up: returns
  * CTB_ERR_TIMEOUT (and adds 1 to the count) with the device still usable. */
 int ctb_diag_bounded_wait(int device, unsigned limit);
+
+/* Diagnostic of the backprojector's overflow path: from the next launch on,
+ * the shared-memory backprojector (single scans and batches) reads every view
+ * whose index is a multiple of `every` through global memory, the path taken by
+ * views whose footprint does not fit the staged box. The result must not
+ * change; 0 turns it off. Process-wide. No reference counterpart. */
+void ctb_diag_force_overflow(int every);
 
 /* ------------------------------------------------------ projection images */
 

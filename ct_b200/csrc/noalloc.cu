@@ -19,13 +19,21 @@
 //  * the array, 256 KB, exists on every GPU that loads the library and stays
 //    there until the process exits;
 //  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress (with that device current) and caches it; make that
-//    first call before any stream capture;
+//    cudaGetSymbolAddress (with that device current) and caches it. With
+//    CUDA's lazy module loading that first lookup is also what loads this
+//    library's kernels onto the device, which takes device memory once, so
+//    make the first call at start-up, before the memory is handed out and
+//    before any stream capture;
+//  * the cached address belongs to the context it was looked up in: it is
+//    kept together with that context's unique ID, and a call that finds a
+//    different context current (after cudaDeviceReset, say) looks it up
+//    again, which again belongs at start-up;
 //  * every call shares the one array and overwrites the entries it uses, so
 //    nothing has to start at zero, but calls whose work overlaps on the GPU
 //    (different streams, or concurrent host threads on the same device) race
 //    on it: serialise them.
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,8 +54,38 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 std::mutex g_addr_mtx;
 void* g_addr[kMaxDevices] = {};
+unsigned long long g_ctx_id[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device (set up once per device).
+// Unique ID of the current context (0 when it cannot be told: no context
+// current yet, or a driver without cuCtxGetId).
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* a = nullptr;
+        void* b = nullptr;
+        cudaDriverEntryPointQueryResult qa, qb;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) == cudaSuccess &&
+            qa == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) == cudaSuccess &&
+            qb == cudaDriverEntryPointSuccess) {
+            get_current = reinterpret_cast<GetCurrent>(a);
+            get_id = reinterpret_cast<GetId>(b);
+        } else {
+            cudaGetLastError();
+        }
+    });
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || get_current(&c) != CUDA_SUCCESS || !c || get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// Device address of the scratch array on the current device: looked up once
+// per device (and again if the device's context was replaced).
 int scratch_address(void** out) {
     int dev = 0;
     CTB_CUDA_TRY(cudaGetDevice(&dev));
@@ -56,7 +94,8 @@ int scratch_address(void** out) {
         return CTB_ERR_UNSUPPORTED;
     }
     std::lock_guard<std::mutex> lk(g_addr_mtx);
-    if (!g_addr[dev]) {
+    const unsigned long long id = current_context_id();
+    if (!g_addr[dev] || (id != 0 && id != g_ctx_id[dev])) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -66,6 +105,7 @@ int scratch_address(void** out) {
             return CTB_ERR_CUDA;
         }
         g_addr[dev] = p;
+        g_ctx_id[dev] = current_context_id();   // the lookup made the context current if it was not
     }
     *out = g_addr[dev];
     return CTB_OK;
@@ -79,10 +119,17 @@ extern "C" int ctb_backproject_noalloc(const void* filtered, int store_type, int
                                        int z_begin, int z_end, float load_scale, float* vol, int accumulate,
                                        void* stream) {
     using namespace ctb;
-    if (!filtered || !vol || !angles_deg || n_views <= 0 || !det || !grid || det->width <= 1 || det->height <= 1 ||
-        !(det->fcd > float(det->width)) || det->radius <= 0 || grid->voxel_pitch <= 0 ||
-        grid->x_to <= grid->x_from || grid->y_to <= grid->y_from || grid->z_to <= grid->z_from) {
+    // the same checks, in the same order, as ctb_backproject
+    if (!filtered || !vol || !angles_deg || n_views <= 0 || !valid_detector(det) || !valid_grid(grid)) {
         set_global_error("ctb_backproject_noalloc: invalid arguments");
+        return CTB_ERR_ARG;
+    }
+    if (z_begin < 0 || z_end <= z_begin || z_end > grid->z_to - grid->z_from) {
+        set_global_error("ctb_backproject_noalloc: invalid z range");
+        return CTB_ERR_ARG;
+    }
+    if (det->radius <= 0) {
+        set_global_error("ctb_backproject_noalloc: detector radius not set (use ctb_reference_grid)");
         return CTB_ERR_ARG;
     }
     if (n_views > kMaxViews) {
@@ -90,10 +137,6 @@ extern "C" int ctb_backproject_noalloc(const void* filtered, int store_type, int
                          std::to_string(kMaxViews) + " views per call; split the views into several calls with "
                          "accumulate = 1, or use ctb_backproject");
         return CTB_ERR_UNSUPPORTED;
-    }
-    if (z_begin < 0 || z_end <= z_begin || z_end > grid->z_to - grid->z_from) {
-        set_global_error("ctb_backproject_noalloc: invalid z range");
-        return CTB_ERR_ARG;
     }
     void* base = nullptr;
     int st = scratch_address(&base);

@@ -78,3 +78,41 @@ def test_noalloc_rejects_more_views_than_its_array():
                                          0, None)
     assert st == L.CTB_ERR_UNSUPPORTED
     assert b"8192" in L.lib().ctb_last_error_global()
+
+
+def test_noalloc_split_views_accumulate_on_a_z_sub_range():
+    """More views than one call should take, split into two calls with
+    accumulate = 1 over a z sub-range, give the one-call ctb_backproject slab."""
+    rng = np.random.default_rng(7)
+    V, H, W, D = 50, 40, 72, 260.0
+    det, grid = ops.detector(W, H, D, u_offset=-0.75)
+    X, Y, Z = grid.box
+    z0, z1 = 9, Z - 5
+    ang = np.sort(rng.uniform(0, 360, V))
+    h = rng.uniform(-2.0, 2.0, V)
+    proj = torch.from_numpy(rng.standard_normal((V, H, W)).astype(np.float32)).cuda()
+    ref = torch.full((z1 - z0, Y, X), float("nan"), device="cuda")
+    assert call("ctb_backproject", proj, L.FP32, ang, h, det, grid, ref, z0, z1) == L.CTB_OK
+    out = torch.zeros((z1 - z0, Y, X), device="cuda")
+    cut = 23
+    for a, b in ((0, cut), (cut, V)):
+        part = proj[a:b].contiguous()
+        assert call("ctb_backproject_noalloc", part, L.FP32, ang[a:b], h[a:b], det, grid, out, z0, z1,
+                    accumulate=1) == L.CTB_OK
+        torch.cuda.synchronize()  # the second call reuses the shared array
+    r = ref.double().cpu().numpy()
+    o = out.double().cpu().numpy()
+    err = np.linalg.norm((o - r).ravel()) / np.linalg.norm(r.ravel())
+    assert err <= 1e-6, err
+
+
+def test_noalloc_rejects_what_the_allocating_entry_point_rejects():
+    det, grid = ops.detector(32, 16, 100.0)
+    proj = torch.zeros((2, 16, 32), device="cuda")
+    out = torch.zeros(grid.box[::-1], device="cuda")
+    bad = L.Grid.from_buffer_copy(grid)
+    bad.x_from = -1
+    ang = np.zeros(2)
+    for name in ("ctb_backproject", "ctb_backproject_noalloc"):
+        assert call(name, proj, L.FP32, ang, None, det, bad, out, 0, grid.box[2]) == L.CTB_ERR_ARG
+        assert call(name, proj, L.FP32, ang, None, det, grid, out, 0, grid.box[2] + 1) == L.CTB_ERR_ARG

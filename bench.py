@@ -118,36 +118,93 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def cpu_baseline(cfg, imgs_sel: np.ndarray, angles_sel, n_views_total, z_slices=16, nthreads=0):
-    """Reference CPU path (oracle restatement) on a bounded sample of the workload.
+# ------------------------------------------------------ reference CPU path
+# The reference's own CPU reconstruction (its Ct/CtVolume.cpp lines compiled
+# unchanged into oracle/_ref/libct_ref.so) on the host cores; the oracle's
+# restatement of it (bit-identical) when that library is absent.
+REF_SAMPLE_VIEWS = 4
+REF_SAMPLE_Z = (0.4375, 0.5625)   # central eighth of the reference grid's slices (its own zmin/zmax)
 
-    Sample: `n_views_sample` views, preprocessed one at a time on one thread (the
-    reference's prefetch thread, Ct/CtVolume.cpp:963-965), and backprojected with
-    all host threads into the full x-y extent of the box over `z_slices` central
-    slices. Scaled to the full workload with the reference's overlap of
-    preprocessing and backprojection: T = V * max(t_pre, t_bp * Z / z_slices)."""
+
+def reference_cpu_available() -> bool:
     from oracle import oracle as orc
-    orc.build()
-    n_views_sample, H, W = imgs_sel.shape
-    V = n_views_total
-    fcd = float(np.float32(cfg["sod"]) / np.float32(cfg["pitch"] * cfg["sod"] / cfg["sdd"]))
-    edge, vs = cfg["edge"], cfg["vs"]
-    z0 = edge // 2 - z_slices // 2
-    g = orc.custom_geom(W, H, fcd, (edge, edge, edge), vs, box=(0, edge, 0, edge, z0, z0 + z_slices))
+    try:
+        orc.ref_lib()
+        return True
+    except (FileNotFoundError, OSError, subprocess.CalledProcessError):
+        return False
+
+
+def cpu_phantom_views(cfg, geom, seed, sel):
+    """uint16 projections of the seeded phantom (the GPU arm's scan of rank 0) for the views `sel`, projected
+    on the CPU (numpy), so the reference arm runs none of the engine."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    from oracle import phantom
+    from ct_b200 import synth
+    rng = np.random.default_rng(seed)
+    r_mm, hz_mm = synth.fov(geom)
+    ell = synth.random_ellipsoids(rng, cfg["n_ell"], r_mm, hz_mm, n_small=cfg["n_small"])
+    ang = geom.angles()[sel]
+    parts = np.array_split(np.arange(len(ang)), min(len(ang), os.cpu_count() or 1))
+    # one process per group of views (spawned: no CUDA state is inherited)
+    with cf.ProcessPoolExecutor(len(parts), mp_context=mp.get_context("spawn")) as ex:
+        futs = [ex.submit(phantom.project, ell, ang[idx], None, geom.width, geom.height, geom.pixel_eff,
+                          geom.sod_mm) for idx in parts]
+        p = np.concatenate([f.result() for f in futs])
+    return synth.intensities_from_line_integrals(p)
+
+
+def reference_cpu_step(cfg, geom, imgs, angles, zrel=REF_SAMPLE_Z, full=False):
+    """One timed run of the reference's CPU path: load the views, set the bounds (x, y whole, z the central
+    slices zrel of the reference grid; `full`: the whole grid), reconstructionCore. Returns the measured
+    wall time and voxel-views of the box it reconstructed."""
+    from oracle import oracle as orc
+    use_ref = reference_cpu_available()
+    rel = None if full else (0.0, 1.0, 0.0, 1.0, zrel[0], zrel[1])
+    ft = FILTERS[cfg["filter"]]
     t0 = time.perf_counter()
-    proj = np.stack([orc.ref_preprocess(im, 1.0, fcd, FILTERS[cfg["filter"]]) for im in imgs_sel])
-    t_pre = (time.perf_counter() - t0) / n_views_sample
-    t0 = time.perf_counter()
-    orc.ref_backproject(proj, np.asarray(angles_sel), np.zeros(n_views_sample), g, nthreads=nthreads)
-    t_bp = (time.perf_counter() - t0) / n_views_sample
-    per_view = max(t_pre, t_bp * edge / z_slices)
-    gups = edge ** 3 / per_view / 1e9
-    cores = orc.num_threads() if nthreads <= 0 else nthreads
-    return {"value": gups, "unit": "GUPS", "cores": cores, "kind": "port",
-            "sample": (f"{n_views_sample} views: preprocessing {t_pre:.3f} s/view on 1 thread, backprojection of "
-                       f"{edge}x{edge}x{z_slices} central slices {t_bp:.3f} s/view on {cores} threads; scaled to "
-                       f"{edge}^3 x {V} views as V*max(t_pre, t_bp*{edge}/{z_slices}) (prefetch overlap)"),
-            "seconds_full_workload_est": per_view * V}
+    if use_ref:
+        # timed inside: the zeroed volume and reconstructionCore, what the reference's
+        # reconstructVolume does for its CPU path (Ct/CtVolume.cpp:553-573)
+        dims, secs = orc.refsrc_reconstruct(imgs, angles, None, geom.pixel_eff, geom.sod_mm, rel=rel,
+                                            filter_type=ft, keep_volume=False)
+    else:
+        FCD = float(np.float32(geom.sod_mm) / np.float32(geom.pixel_eff))
+        g = orc.ref_geom(geom.width, geom.height, FCD, rel=orc.clamp_bounds(*rel) if rel else (0, 1, 0, 1, 0, 1))
+        a, h = orc.fix_sinogram(angles, np.zeros(len(angles)), True, geom.pixel_eff)
+        vol, secs = orc.ref_reconstruct(imgs, a, h, 1.0, ft, g)
+        dims = vol.shape
+        del vol
+    wall = time.perf_counter() - t0
+    units = float(np.prod(dims)) * len(angles)
+    return {"seconds": secs, "call_seconds": wall, "voxel_views": units, "box": list(dims),
+            "kind": "reference" if use_ref else "port", "cores": orc.num_threads()}
+
+
+def reference_c1_full(seed=1000):
+    """The reference's CPU path on the whole 360-view scan of 256 x 192 into its 252^2 x 192 grid, measured."""
+    cfg = CONFIGS["c1"]
+    geom = geometry(cfg)
+    imgs = cpu_phantom_views(cfg, geom, seed, np.arange(geom.n_views))
+    r = reference_cpu_step(cfg, geom, imgs, geom.angles(), full=True)
+    return {"workload": "360 views x 256x192 u16 -> 252x252x192 f32 (reference grid), ramlak", "seconds": r["seconds"],
+            "gups": r["voxel_views"] / r["seconds"] / 1e9, "kind": r["kind"], "cores": r["cores"]}
+
+
+def cpu_baseline(cfg, geom, imgs_sel, angles_sel, units_full):
+    """The reference's CPU path on a bounded sample of the workload, measured: REF_SAMPLE_VIEWS evenly spaced
+    views of this scan reconstructed by the reference's own code into the central slices of its own grid
+    (voxel = 1 detector pixel; it has no coarser voxels). value = voxel-views per second of that run."""
+    r = reference_cpu_step(cfg, geom, imgs_sel, angles_sel)
+    gups = r["voxel_views"] / r["seconds"] / 1e9
+    X, Y, Z = r["box"]
+    return {"value": gups, "unit": "GUPS", "cores": r["cores"], "kind": r["kind"],
+            "sample": (f"{len(angles_sel)} of {geom.n_views} views, reference grid box {X}x{Y}x{Z} (z "
+                       f"{REF_SAMPLE_Z[0]}..{REF_SAMPLE_Z[1]}): {r['seconds']:.2f} s for the zeroed volume and "
+                       f"reconstructionCore ({r['call_seconds']:.2f} s with loading) on {r['cores']} threads"),
+            "seconds": r["seconds"],
+            "seconds_full_workload_at_this_rate": units_full / (gups * 1e9)}
 
 
 def log(*a):
@@ -180,6 +237,17 @@ def fp64_reference_slices(rows, cfg, geom, det, grid, z0, z1):
                         box=(grid.x_from, grid.x_to, grid.y_from, grid.y_to, grid.z_from, grid.z_to))
     ref = orc.f64_slices(rows, r0, H, geom.angles(), np.zeros(V), 1.0, FILTERS[cfg["filter"]], g, z0, z1)
     return ref  # (x, y, z1 - z0)
+
+
+def accuracy_slices(Z):
+    """Slices scored against the FP64 oracle: both ends (largest cone angle), the octiles and the centre."""
+    return sorted({0, Z // 8, Z // 4, Z // 2 - 1, Z // 2, 3 * Z // 4, 7 * Z // 8, Z - 1})
+
+
+def fp64_slice_set(raw, cfg, geom, det, grid, zs):
+    """FP64 oracle values of the box slices zs, each from only the detector rows it touches: (x, y, len(zs))."""
+    return np.concatenate([fp64_reference_slices(oracle_rows(raw, geom, det, grid, z, z + 1), cfg, geom, det, grid,
+                                                 z, z + 1) for z in zs], axis=2)
 
 
 def accuracy(vol_slices_zyx, ref_xyz):
@@ -286,6 +354,59 @@ def batch_c5(n_scans=32, seed=5, store="fp16", reps=3):
     return out
 
 
+# ------------------------------------------------------------ C2 (FP32)
+def c2_leg(reps=3, with_accuracy=True):
+    """C2: 720 views of 1024 x 1024 (0.4 mm pitch, SOD 500, SDD 1000), 30 seeded ellipsoids with Poisson
+    noise at 1e5 photons, shepplogan, FP32 storage, into 512^3 (voxel 2 detector pixels) and into the
+    0.25..0.75 sub-box (256^3). Device time (filter + backprojection, CUDA events) and rel-L2 / max-abs of
+    eight slices per box against the FP64 oracle."""
+    import torch
+
+    from ct_b200 import ops, synth
+    from ct_b200 import _lib as L
+    cfg = CONFIGS["c2"]
+    geom = geometry(cfg)
+    V, W, H, edge, vs = geom.n_views, geom.width, geom.height, cfg["edge"], cfg["vs"]
+    ft = FILTERS[cfg["filter"]]
+    scan = synth.make_scan(geom, cfg["n_ell"], seed=2000, photons=cfg["photons"], n_small=cfg["n_small"])
+    raw, angles = scan.images, geom.angles()
+    det, _ = ops.detector(W, H, geom.fcd_px)
+    stream = torch.cuda.current_stream()
+    out = {"workload": f"c2: {V} views x {W}x{H} u16 -> {edge}^3 f32 (voxel {vs} px), {cfg['filter']}, fp32 storage, "
+                       f"Poisson 1e5"}
+    filtered = torch.empty((V, H, W), dtype=torch.float32, device="cuda")
+    for name, rel in (("full", (0.0, 1.0)), ("subbox_0.25_0.75", (0.25, 0.75))):
+        lo, hi = int(rel[0] * edge + 0.5), int(rel[1] * edge + 0.5)
+        grid = ops.custom_grid(det, (edge, edge, edge), vs, box=(lo, hi, lo, hi, lo, hi))
+        X, Y, Z = grid.box
+        vol = torch.empty((Z, Y, X), dtype=torch.float32, device="cuda")
+
+        def step():
+            ops.filter_projections(raw, det, ft, 1, L.FP32, 1.0, out=filtered)
+            ops.backproject(filtered, angles, None, det, grid, out=vol)
+
+        step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        r = {"volume": [X, Y, Z], "ms": ms, "gups": float(X) * Y * Z * V / (ms * 1e-3) / 1e9}
+        if with_accuracy:
+            zs = accuracy_slices(Z)
+            got = vol[torch.tensor(zs, device="cuda")].cpu().numpy()
+            ref = fp64_slice_set(raw, cfg, geom, det, grid, zs)
+            r["accuracy_vs_fp64"] = {"slices": zs, "fp32": accuracy(got, ref)}
+        out[name] = r
+        del vol
+    del filtered, raw, scan
+    torch.cuda.empty_cache()
+    return out
+
+
 # ------------------------------------------------------- differentiation (C4)
 def voxelise_gpu(ellipsoids, edge, voxel_mm):
     """Phantom density at the voxel centres of an edge^3 grid centred on the axis, (Z, Y, X) float32."""
@@ -308,9 +429,11 @@ def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
     512x512. Dot-product test <Ax, y> = <x, A^T y> with seeded Gaussian x, y; device time of A and A^T;
     central finite differences of f(x) = ||Ax - p||^2 on 64 random voxels against 2 A^T (Ax - p)
     (A(x +- eps e_i) = Ax +- eps A e_i, with A e_i projected from a one-slice slab holding the voxel);
-    then 20 steepest-descent iterations with exact line search. The data are consistent with the model:
-    p = A(truth) + 1 % Gaussian noise, truth the voxelised 20-ellipsoid phantom; the start is the FDK
-    reconstruction (hann) of the phantom's analytic projections (Poisson noise at 1e4 photons), scaled to p."""
+    then 20 steepest-descent iterations with exact line search from the FDK reconstruction.
+    Data as the configuration states them: the analytic projections of a 20-ellipsoid phantom with Poisson
+    noise at 1e4 photons, as line integrals in voxel lengths (-ln(I / I0) / 0.02 / voxel mm; with the U^2
+    weight, A of a density is its line integral in voxel lengths). The same descent on model-consistent
+    data (A of the voxelised phantom + 1 % Gaussian noise) is reported beside it."""
     import torch
 
     from ct_b200 import ops, synth
@@ -343,64 +466,92 @@ def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
     fp_ms, bp_ms = ev[0].elapsed_time(ev[1]) / reps, ev[1].elapsed_time(ev[2]) / reps
     out.update({"forward_ms": fp_ms, "forward_gups": units / fp_ms / 1e6,
                 "backproject_fp32_ms": bp_ms, "backproject_fp32_gups": units / bp_ms / 1e6})
-    del Ax, Aty, y
-    # data consistent with the model: A(truth) + noise
+    del Ax, Aty, y, x
     scan = synth.make_scan(geom, 20, seed=seed, photons=1e4)
-    truth = voxelise_gpu(scan.ellipsoids, edge, geom.pixel_eff)
-    p = ops.forward_project(truth, ang, None, d, grid)
-    p.add_(torch.randn(p.shape, device="cuda", generator=g), alpha=0.01 * float(p.double().pow(2).mean().sqrt()))
-    # FDK start (hann, FP32) from the analytic noisy projections, scaled to the data by least squares
+    voxel_mm = geom.pixel_eff
+    truth = voxelise_gpu(scan.ellipsoids, edge, voxel_mm)
+    # FDK (hann, FP32) of the noisy analytic projections
     filt = ops.filter_projections(scan.images, d, L.HANN, 1, L.FP32)
-    x = ops.backproject(filt, ang, None, d, grid)
+    fdk = ops.backproject(filt, ang, None, d, grid)
     del filt
-    Ax = ops.forward_project(x, ang, None, d, grid)
-    c = float((Ax.double() * p.double()).sum() / (Ax.double() * Ax.double()).sum())
-    x.mul_(c)
-    r = Ax.mul_(c).sub_(p)
 
     def err_to_truth(v):
         vs = v.double()
         s_fit = float((vs * truth).sum() / (vs * vs).sum())
         return float((s_fit * vs - truth).norm() / truth.norm())
 
-    # finite differences on 64 voxels
-    grad = 2.0 * ops.backproject(r, ang, None, d, grid)
-    rng = np.random.default_rng(seed)
-    eps, worst = 1.0, 0.0
-    for _ in range(64):
-        k, j, i = (int(rng.integers(edge // 4, 3 * edge // 4)) for _ in range(3))
-        slab = torch.zeros((1, edge, edge), device="cuda")
-        slab[0, j, i] = 1.0
-        Ae = ops.forward_project(slab, ang, None, d, grid, k, k + 1).double()
-        rd = r.double()
-        fp = float(((rd + eps * Ae) ** 2).sum())
-        fm = float(((rd - eps * Ae) ** 2).sum())
-        fd = (fp - fm) / (2 * eps)
-        gi = float(grad[k, j, i])
-        worst = max(worst, abs(fd - gi) / max(abs(fd), 1e-12))
-    del grad
-    out["fd_max_rel_err_64_voxels"] = worst
-    # steepest descent with exact line search on the quadratic
-    res0 = float(r.double().norm() / p.double().norm())
-    err0 = err_to_truth(x)
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    for _ in range(iters):
-        gk = 2.0 * ops.backproject(r, ang, None, d, grid)
-        Ag = ops.forward_project(gk, ang, None, d, grid)
-        alpha = float((gk.double() ** 2).sum() / (2.0 * (Ag.double() ** 2).sum()))
-        x.sub_(alpha * gk)
-        r.sub_(alpha * Ag)
-        del gk, Ag
-    torch.cuda.synchronize()
-    t_it = (time.perf_counter() - t1) / iters
-    res = float(r.double().norm() / p.double().norm())
-    out.update({"data_residual_rel_start": res0, "data_residual_rel_after": res, "iterations": iters,
-                "rel_l2_to_phantom_start": err0, "rel_l2_to_phantom_after": err_to_truth(x),
-                "seconds_per_iteration": t_it, "seconds_total": time.perf_counter() - t0})
-    del x, r, p, truth, scan
+    def descend(p, fd_check):
+        """Steepest descent on ||Ax - p||^2 from the FDK volume scaled to p by least squares."""
+        x = fdk.clone()
+        Ax = ops.forward_project(x, ang, None, d, grid)
+        c = float((Ax.double() * p.double()).sum() / (Ax.double() * Ax.double()).sum())
+        x.mul_(c)
+        r = Ax.mul_(c).sub_(p)
+        res = {}
+        if fd_check:
+            grad = 2.0 * ops.backproject(r, ang, None, d, grid)
+            rng = np.random.default_rng(seed)
+            eps, worst = 1.0, 0.0
+            for _ in range(64):
+                k, j, i = (int(rng.integers(edge // 4, 3 * edge // 4)) for _ in range(3))
+                slab = torch.zeros((1, edge, edge), device="cuda")
+                slab[0, j, i] = 1.0
+                Ae = ops.forward_project(slab, ang, None, d, grid, k, k + 1).double()
+                rd = r.double()
+                fp = float(((rd + eps * Ae) ** 2).sum())
+                fm = float(((rd - eps * Ae) ** 2).sum())
+                fd = (fp - fm) / (2 * eps)
+                gi = float(grad[k, j, i])
+                worst = max(worst, abs(fd - gi) / max(abs(fd), 1e-12))
+            del grad
+            res["fd_max_rel_err_64_voxels"] = worst
+        res0 = float(r.double().norm() / p.double().norm())
+        err0 = err_to_truth(x)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(iters):
+            gk = 2.0 * ops.backproject(r, ang, None, d, grid)
+            Ag = ops.forward_project(gk, ang, None, d, grid)
+            alpha = float((gk.double() ** 2).sum() / (2.0 * (Ag.double() ** 2).sum()))
+            x.sub_(alpha * gk)
+            r.sub_(alpha * Ag)
+            del gk, Ag
+        torch.cuda.synchronize()
+        t_it = (time.perf_counter() - t1) / iters
+        res.update({"data_residual_rel_start": res0, "data_residual_rel_after": float(r.double().norm() /
+                                                                                       p.double().norm()),
+                    "iterations": iters, "rel_l2_to_phantom_start": err0, "rel_l2_to_phantom_after": err_to_truth(x),
+                    "seconds_per_iteration": t_it})
+        del x, r
+        return res
+
+    # the configuration's data: analytic Poisson-1e4 projections as line integrals in voxel lengths
+    p = (-torch.log(scan.images.float().clamp_min(1.0) / 65535.0) / 0.02 / voxel_mm).contiguous()
+    a = descend(p, fd_check=True)
+    out["fd_max_rel_err_64_voxels"] = a.pop("fd_max_rel_err_64_voxels")
+    out["analytic_poisson_1e4"] = a
+    # model-consistent data: A(truth) + 1 % Gaussian noise
+    p = ops.forward_project(truth, ang, None, d, grid)
+    p.add_(torch.randn(p.shape, device="cuda", generator=g), alpha=0.01 * float(p.double().pow(2).mean().sqrt()))
+    out["model_consistent"] = descend(p, fd_check=False)
+    out["seconds_total"] = time.perf_counter() - t0
+    del p, truth, scan, fdk
     torch.cuda.empty_cache()
     return out
+
+
+def workload_config(args, world):
+    """The `config` object of the bench line (both arms print the same one)."""
+    cfg = CONFIGS[args.config]
+    V, W, H, edge, vs = cfg["views"], cfg["W"], cfg["H"], cfg["edge"], cfg["vs"]
+    rel = (0.25, 0.75) if args.subbox else (0.0, 1.0)
+    n = int(rel[1] * edge + 0.5) - int(rel[0] * edge + 0.5)
+    return {"workload": f"{args.config}: {V} views x {W}x{H} u16 -> {n}x{n}x{n} f32 (voxel {vs} px), "
+                        f"{cfg['filter']}, {args.store} storage"
+                        + (f", sub-box 0.25..0.75 of {edge}^3" if args.subbox else ""),
+            "storage": args.store, "views": V, "detector": [W, H], "volume": [n, n, n], "voxel_pitch_px": vs,
+            "slab": args.slab, "l2": f"inputs ({V * H * W * 2 / 1e9:.1f} GB raw) larger than L2 (126 MB); no flush",
+            "parallelism": f"replicas{world}"}
 
 
 # ------------------------------------------------------------------ our arm
@@ -472,34 +623,39 @@ def run_ours(args):
         b_ms = float(np.mean([e[1].elapsed_time(e[2]) for e in evs]))
         out = {"total_ms": max_over_ranks(total_ms, world), "filter_ms": f_ms, "bp_ms": b_ms, "clocks": clocks}
         del filtered
-        zc = Z // 2
-        centre = vol[zc - 1:zc + 1].cpu().numpy()
+        sel = vol[torch.tensor(acc_z, device="cuda")].cpu().numpy()
         del vol
         torch.cuda.empty_cache()
-        return out, centre
+        return out, sel
 
+    acc_z = accuracy_slices(Z)
     log(f"scan ready: {V} views {W}x{H} -> {X}x{Y}x{Z}")
-    main, centre = timed(store, args.steps, args.warmup)
+    main, slices_main = timed(store, args.steps, args.warmup)
     ms_per_step = main["total_ms"] / args.steps
     value = whole_job_gups(units, world, ms_per_step)
     log(f"{args.store}: {ms_per_step:.1f} ms/step, {value:.1f} GUPS, filter {main['filter_ms']:.1f} ms, "
         f"bp {main['bp_ms']:.1f} ms, clocks {main['clocks']}")
 
     # plain FP32 path on the same workload (mixed vs plain ratio)
-    fp32, centre32 = None, None
+    fp32, slices32 = None, None
     if store != L.FP32 and not args.skip_fp32:
-        r32, centre32 = timed(L.FP32, max(2, args.steps // 2), 1)
+        r32, slices32 = timed(L.FP32, max(2, args.steps // 2), 1)
         ms32 = r32["total_ms"] / max(2, args.steps // 2)
         fp32 = {"value": whole_job_gups(units, world, ms32), "ms_per_step": ms32, "bp_ms": r32["bp_ms"],
                 "filter_ms": r32["filter_ms"]}
         log(f"fp32: {fp32}")
+    # the other 16-bit storage type on the same workload
+    other = {L.FP16: ("bf16", L.BF16), L.BF16: ("fp16", L.FP16)}.get(store)
+    alt, slices_alt = None, None
+    if other and not args.skip_fp32:
+        ra, slices_alt = timed(other[1], max(2, args.steps // 2), 1)
+        msa = ra["total_ms"] / max(2, args.steps // 2)
+        alt = {"value": whole_job_gups(units, world, msa), "ms_per_step": msa, "bp_ms": ra["bp_ms"],
+               "filter_ms": ra["filter_ms"]}
+        log(f"{other[0]}: {alt}")
 
-    # the central slices' FP64-oracle accuracy is computed in the CPU leg below
+    # the FP64-oracle accuracy of these slices is computed in the CPU leg below
     acc = None
-    zc = Z // 2
-    rows_for_oracle = None
-    if rank == 0 and world == 1 and not args.skip_cpu and not args.skip_accuracy:
-        rows_for_oracle = oracle_rows(raw, geom, det, grid, zc - 1, zc + 1)
 
     # end to end through the C ABI facade: pinned host u16 -> pinned host float volume
     e2e = None
@@ -534,6 +690,10 @@ def run_ours(args):
         del v, host_in, host_out
         log(f"e2e: {e2e}")
 
+    c2 = None
+    if not args.skip_c2 and args.config == "c3":
+        c2 = c2_leg(with_accuracy=rank == 0 and world == 1 and not args.skip_accuracy)
+        log(f"c2: {c2}")
     batch = None
     if not args.skip_batch and args.config == "c3":
         batch = batch_c5(store=args.store)
@@ -570,16 +730,14 @@ def run_ours(args):
         "metric": "FDK GUPS (voxels x views / s)", "value": value, "unit": "GUPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.config}: {V} views x {W}x{H} u16 -> {X}x{Y}x{Z} f32 (voxel {vs} px), "
-                               f"{cfg['filter']}, {args.store} storage"
-                               + (f", sub-box 0.25..0.75 of {edge}^3" if args.subbox else ""), "storage": args.store,
-                   "views": V, "detector": [W, H], "volume": [X, Y, Z], "voxel_pitch_px": vs,
-                   "slab": slab, "l2": f"inputs ({V * H * W * 2 / 1e9:.1f} GB raw) larger than L2 (126 MB); no flush", "parallelism": f"replicas{world}"},
+        "config": workload_config(args, world),
         "recon_seconds": ms_per_step * 1e-3,
         "stage_ms": {"filter": main["filter_ms"], "backproject": main["bp_ms"]},
         "fp32": fp32,
         "mixed_over_fp32": (value / fp32["value"]) if fp32 else None,
+        (other[0] if other else "other_storage"): alt,
         "accuracy_vs_fp64": acc,
+        "c2_fp32": c2,
         "batch_c5": batch,
         "gradient_c4": grad,
         "e2e": e2e,
@@ -591,14 +749,23 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.skip_cpu:
         # CPU leg: the reference's CPU path on a bounded sample (baseline) and the FP64
         # oracle on the central slices (accuracy of this run's volumes)
-        sel = np.linspace(0, V - 1, 8).astype(int)
+        sel = np.linspace(0, V - 1, REF_SAMPLE_VIEWS).astype(int)
         imgs_sel = torch.stack([raw[int(i)] for i in sel]).to(torch.int32).cpu().numpy().astype(np.uint16)
-        line["cpu_baseline"] = cpu_baseline(cfg, imgs_sel, angles[sel], V)
-        if rows_for_oracle is not None:
-            ref = fp64_reference_slices(rows_for_oracle, cfg, geom, det, grid, zc - 1, zc + 1)
-            acc = {"slices": [zc - 1, zc + 1], args.store: accuracy(centre, ref)}
-            if centre32 is not None:
-                acc["fp32"] = accuracy(centre32, ref)
+        line["cpu_baseline"] = cpu_baseline(cfg, geom, imgs_sel, angles[sel], units)
+        line["cpu_baseline"]["c1_full"] = reference_c1_full()
+        log(f"cpu baseline: {line['cpu_baseline']}")
+        if not args.skip_accuracy:
+            t0 = time.perf_counter()
+            ref = fp64_slice_set(raw, cfg, geom, det, grid, acc_z)
+            acc = {"slices": acc_z, args.store: accuracy(slices_main, ref)}
+            if slices_alt is not None:
+                acc[other[0]] = accuracy(slices_alt, ref)
+            if slices32 is not None:
+                acc["fp32"] = accuracy(slices32, ref)
+            # per slice, the mixed-precision storage
+            acc["per_slice_rel_l2_" + args.store] = [accuracy(slices_main[i:i + 1], ref[:, :, i:i + 1])["rel_l2"]
+                                                     for i in range(len(acc_z))]
+            acc["oracle_seconds"] = time.perf_counter() - t0
             line["accuracy_vs_fp64"] = acc
             log(f"accuracy: {acc}")
     if rank == 0:
@@ -610,43 +777,45 @@ def run_ours(args):
 
 # ----------------------------------------------------------- reference arm
 def run_reference(args):
-    """The reference's CPU reconstruction path (oracle restatement; the reference
-    itself needs Qt5 + OpenCV C++ and is not buildable here) on the host cores,
-    each step a bounded sample of the same workload."""
+    """The reference's own CPU reconstruction code (oracle/_ref: its Ct/CtVolume.cpp lines compiled unchanged;
+    the reference application itself needs Qt5 and the OpenCV C++ API, absent here) on all host cores. Each
+    step is a measured run on a bounded sample of the same workload: REF_SAMPLE_VIEWS views of the same seeded
+    phantom reconstructed into the central slices of the reference's own grid. ms_per_step is that run's wall
+    time and value its voxel-views per second; the full workload's time at that rate is a separate field."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cfg = CONFIGS[args.config]
     geom = geometry(cfg)
-    V, W, H = geom.n_views, geom.width, geom.height
-    # the same phantom family, projected on the CPU for the sampled views only
-    from oracle import phantom
-    from ct_b200 import synth
-    rng = np.random.default_rng(1000)
-    r_mm, hz_mm = synth.fov(geom)
-    ell = synth.random_ellipsoids(rng, cfg["n_ell"], r_mm, hz_mm, n_small=cfg["n_small"])
-    angles = geom.angles()
-    n_s = 8
-    sel = np.linspace(0, V - 1, n_s).astype(int)
-    p = phantom.project(ell, angles[sel], None, W, H, geom.pixel_eff, geom.sod_mm)
-    imgs = synth.intensities_from_line_integrals(p)
-    vals = []
+    V = geom.n_views
+    sel = np.linspace(0, V - 1, REF_SAMPLE_VIEWS).astype(int)
+    imgs = cpu_phantom_views(cfg, geom, scan_seed(0), sel)
+    angles = geom.angles()[sel]
+    runs = []
     for k in range(args.warmup + args.steps):
-        r = cpu_baseline(cfg, imgs, angles[sel], V)
+        r = reference_cpu_step(cfg, geom, imgs, angles)
         if k >= args.warmup:
-            vals.append(r)
-    value = float(np.mean([r["value"] for r in vals]))
-    last = vals[-1]
+            runs.append(r)
+    secs = float(np.mean([r["seconds"] for r in runs]))
+    value = runs[0]["voxel_views"] / secs / 1e9
+    conf = workload_config(args, world)
+    n = conf["volume"][0]
+    units_full = float(n) ** 3 * V
+    X, Y, Z = runs[0]["box"]
+    sample = (f"{REF_SAMPLE_VIEWS} of {V} views of the seeded phantom (CPU-projected), reference grid box "
+              f"{X}x{Y}x{Z} (z {REF_SAMPLE_Z[0]}..{REF_SAMPLE_Z[1]}; voxel = 1 detector pixel, the reference has "
+              f"no coarser voxels), {runs[0]['cores']} threads, {cfg['filter']}")
     line = {"metric": "FDK GUPS (voxels x views / s)", "value": value, "unit": "GUPS", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": last["seconds_full_workload_est"] * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": f"{args.config}: {V} views x {W}x{H} u16 -> {cfg['edge']}^3 f32, "
-                                   f"{cfg['filter']}, reference CPU path"},
-            "cpu_baseline": {"value": value, "unit": "GUPS", "cores": last["cores"], "kind": "port",
-                             "sample": last["sample"]},
-            "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "impl": "reference", "config": conf,
+            "cpu_baseline": {"value": value, "unit": "GUPS", "cores": runs[0]["cores"], "kind": runs[0]["kind"],
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "extrapolated": {"seconds_full_workload_at_measured_rate": units_full / (value * 1e9),
+                             "note": f"{n}^3 x {V} voxel-views at this run's rate"},
+            "c1_full": reference_c1_full()}
     print(json.dumps(line), flush=True)
 
 
@@ -666,6 +835,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
+    ap.add_argument("--skip-c2", action="store_true")
     ap.add_argument("--skip-gradient", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

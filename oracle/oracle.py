@@ -273,7 +273,7 @@ def ref_lib(variant: str = "msvc"):
         P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
         L.ref_reconstruct.restype = I
         L.ref_reconstruct.argtypes = [P, I, I, I, I, P, P, D, D, D, D, ctypes.c_char_p, P, I, ctypes.c_uint, P, P,
-                                      P]
+                                      P, I]
         L.ref_prepare_projection.restype = I
         L.ref_prepare_projection.argtypes = [P, I, I, I, I, P, D, D, D, I, I, P]
         L.ref_fix_sinogram.restype = I
@@ -285,11 +285,12 @@ def ref_lib(variant: str = "msvc"):
 def refsrc_reconstruct(imgs: np.ndarray, angles_deg, heights_mm, pixel_size: float, fcd_mm: float,
                        u_offset_mm: float = 0.0, base: float = 1.0, rotation: str = "ccw", rel=None,
                        filter_type: int = RAMLAK, skip: int = 0, dims_only: bool = False,
-                       variant: str = "msvc"):
+                       variant: str = "msvc", keep_volume: bool = True):
     """The reference's own CPU reconstruction (CSV values as they appear in the
     file: angles in degrees, heights and distances in mm). Returns
-    (volume (x, y, z) Z_FASTEST, seconds of reconstructionCore), or the box
-    dimensions with dims_only."""
+    (volume (x, y, z) Z_FASTEST, seconds of the zeroed volume and
+    reconstructionCore), or the box dimensions with dims_only. keep_volume=False
+    runs the reconstruction and returns (box dimensions, seconds)."""
     imgs = np.ascontiguousarray(imgs)
     V, H, W = imgs.shape
     a = np.ascontiguousarray(angles_deg, np.float64)
@@ -299,14 +300,19 @@ def refsrc_reconstruct(imgs: np.ndarray, angles_deg, heights_mm, pixel_size: flo
     L = ref_lib(variant)
     args = (_p(imgs), _depth(imgs[0]), V, W, H, _p(a), None if h is None else _p(h), pixel_size, u_offset_mm,
             fcd_mm, base, rotation.encode(), None if r6 is None else _p(r6), filter_type, skip)
-    st = L.ref_reconstruct(*args, None, _p(dims), None)
+    st = L.ref_reconstruct(*args, None, _p(dims), None, 0)
     if st != 0:
         raise RuntimeError(f"ref_reconstruct failed ({st})")
     if dims_only:
         return tuple(int(d) for d in dims)
-    vol = np.zeros(tuple(int(d) for d in dims), np.float32)
     secs = ctypes.c_double(0)
-    st = L.ref_reconstruct(*args, _p(vol), _p(dims), ctypes.byref(secs))
+    if not keep_volume:
+        st = L.ref_reconstruct(*args, None, _p(dims), ctypes.byref(secs), 1)
+        if st != 0:
+            raise RuntimeError(f"ref_reconstruct failed ({st})")
+        return tuple(int(d) for d in dims), secs.value
+    vol = np.zeros(tuple(int(d) for d in dims), np.float32)
+    st = L.ref_reconstruct(*args, _p(vol), _p(dims), ctypes.byref(secs), 1)
     if st != 0:
         raise RuntimeError(f"ref_reconstruct failed ({st})")
     return vol, secs.value

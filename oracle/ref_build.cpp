@@ -214,12 +214,15 @@ extern "C" {
 // relative heights in mm, angle direction "cw"/"ccw", grid rule), bounds
 // rel6 = {xmin, xmax, ymin, ymax, zmin, zmax} (NULL: whole grid), filter
 // 0/1/2, skip projections, then reconstructionCore into a Z_FASTEST volume.
-// dims receives xMax, yMax, zMax; with vol == NULL only dims are set.
-// seconds: steady-clock time of reconstructionCore. Returns 0 on success.
+// dims receives xMax, yMax, zMax. With vol == NULL and run == 0 only dims are
+// set; with vol == NULL and run != 0 the reconstruction runs and its volume is
+// dropped. seconds: steady-clock time of what reconstructVolume does for the
+// CPU path (:553-573): the zeroed volume (reinitialise) and reconstructionCore.
+// Returns 0 on success.
 int ref_reconstruct(const void* images, int bits, int n_views, int W, int H, const double* angles_deg,
                     const double* heights_mm, double pixel_size, double u_offset_mm, double fcd_mm, double base,
                     const char* rotation, const float* rel6, int filter, unsigned skip, float* vol, int* dims,
-                    double* seconds) {
+                    double* seconds, int run) {
     QuietCout quiet;
     ct::CtVolume c;
     try {
@@ -231,14 +234,14 @@ int ref_reconstruct(const void* images, int bits, int n_views, int W, int H, con
         dims[0] = int(c.xMax);
         dims[1] = int(c.yMax);
         dims[2] = int(c.zMax);
-        if (!vol) return 0;
-        c.volume.reinitialise(c.xMax, c.yMax, c.zMax, 0);
+        if (!vol && !run) return 0;
         const auto t0 = std::chrono::steady_clock::now();
+        c.volume.reinitialise(c.xMax, c.yMax, c.zMax, 0);
         const bool ok = c.reconstructionCore();
         const auto t1 = std::chrono::steady_clock::now();
         if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
         if (!ok) return 2;
-        std::memcpy(vol, c.volume.data(), c.volume.size() * sizeof(float));
+        if (vol) std::memcpy(vol, c.volume.data(), c.volume.size() * sizeof(float));
     } catch (const std::exception&) {
         return 1;
     }

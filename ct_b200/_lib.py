@@ -9,7 +9,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libctb.so")
+# CTB_LIBRARY=checked loads the bounds-checked build (libctb_checked.so,
+# kernels compiled with CTB_BOUNDS_CHECK) instead of libctb.so.
+LIB_PATH = os.path.join(HERE, "libctb_checked.so" if os.environ.get("CTB_LIBRARY") == "checked" else "libctb.so")
 
 # status codes
 CTB_OK, CTB_ERR_ARG, CTB_ERR_IO, CTB_ERR_CSV, CTB_ERR_IMAGE, CTB_ERR_ALLOC, CTB_ERR_CUDA, CTB_ERR_TIMEOUT, \
@@ -77,6 +79,12 @@ SIGNATURES = {
     "ctb_backproject_noalloc": (I, [P, I, I, P, P, P, P, I, I, F, P, I, P]),
     "ctb_forward_project": (I, [P, P, P, I, P, P, I, I, P, I, P]),
     "ctb_diag_force_overflow": (None, [I]),
+    "ctb_diag_fail_allocation": (None, [ctypes.c_long]),
+    "ctb_diag_bounds_status": (I, [I, P, P, P, I]),
+    "ctb_forward": (I, [P, P, P]),
+    "ctb_backward": (I, [P, P, P]),
+    "ctb_gradient": (I, [P, P, P, P, P]),
+    "ctb_batch_reconstruct": (I, [P, I, P, P]),
     "ctb_convert_layout": (I, [P, I, I, I, I, I, P, P]),
     "ctb_create": (I, [P]),
     "ctb_destroy": (None, [P]),
@@ -149,7 +157,8 @@ def lib():
     global _lib
     if _lib is None:
         if not os.path.exists(LIB_PATH):
-            raise RuntimeError(f"libctb.so not found at {LIB_PATH}; build it with `python -m ct_b200.build`")
+            raise RuntimeError(f"{os.path.basename(LIB_PATH)} not found at {LIB_PATH}; build it with "
+                               "`python -m ct_b200.build`")
         L = ctypes.CDLL(LIB_PATH)
         for name, (res, args) in SIGNATURES.items():
             fn = getattr(L, name)

@@ -4,7 +4,9 @@
     python -m ct_b200.build --clean
 
 Objects go to ct_b200/_build/, the library to ct_b200/libctb.so and the CLI
-to ct_b200/ctb. Everything is compiled for sm_100a only.
+to ct_b200/ctb; the bounds-checked library (CTB_BOUNDS_CHECK) to
+ct_b200/libctb_checked.so from ct_b200/_build_checked/. Everything is compiled
+for sm_100a only.
 """
 from __future__ import annotations
 
@@ -41,14 +43,21 @@ SOURCES = [
     "host/tables.cpp",
     "host/batch.cpp",
     "host/volume_reader.cpp",
+    "host/operators.cpp",
     "capi.cpp",
     "noalloc.cu",
 ]
 HEADERS = ["ctb_internal.h", "host/reconstructor.h", "host/image_io.h", "host/autotune.h", "kernels/geom.cuh"]
 
 
-def _obj(src: str) -> str:
-    return os.path.join(BUILD, src.replace("/", "_") + ".o")
+# The bounds-checked library (kernels check every texel fetch, see
+# ctb_diag_bounds_status) is built from the same sources with CTB_BOUNDS_CHECK.
+CHECKED_BUILD = os.path.join(HERE, "_build_checked")
+CHECKED_LIB = os.path.join(HERE, "libctb_checked.so")
+
+
+def _obj(src: str, checked: bool = False) -> str:
+    return os.path.join(CHECKED_BUILD if checked else BUILD, src.replace("/", "_") + ".o")
 
 
 def _newer(target: str, deps) -> bool:
@@ -58,13 +67,15 @@ def _newer(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def _compile(src: str, verbose: bool) -> str:
+def _compile(src: str, verbose: bool, checked: bool = False) -> str:
     path = os.path.join(CSRC, src)
-    obj = _obj(src)
+    obj = _obj(src, checked)
     deps = [path, os.path.join(ROOT, "include", "ctb.h")] + [os.path.join(CSRC, h) for h in HEADERS]
     if not _newer(obj, deps):
         return obj
     flags = CU_FLAGS if src.endswith(".cu") else ARCH + COMMON
+    if checked:
+        flags = flags + ["-DCTB_BOUNDS_CHECK"]
     cmd = [NVCC] + flags + ["-c", path, "-o", obj]
     if verbose:
         print(" ".join(cmd), flush=True)
@@ -76,17 +87,21 @@ def _compile(src: str, verbose: bool) -> str:
     return obj
 
 
-def build(verbose: bool = False, clean: bool = False) -> str:
-    if clean and os.path.isdir(BUILD):
-        shutil.rmtree(BUILD)
-    os.makedirs(BUILD, exist_ok=True)
-    with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
-        objs = list(ex.map(lambda s: _compile(s, verbose), SOURCES))
-    if _newer(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lz", "-lpthread"]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+def build(verbose: bool = False, clean: bool = False, checked: bool = True) -> str:
+    if clean:
+        for d in (BUILD, CHECKED_BUILD):
+            if os.path.isdir(d):
+                shutil.rmtree(d)
+    variants = [(False, BUILD, LIB)] + ([(True, CHECKED_BUILD, CHECKED_LIB)] if checked else [])
+    for chk, bdir, lib in variants:
+        os.makedirs(bdir, exist_ok=True)
+        with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+            objs = list(ex.map(lambda s: _compile(s, verbose, chk), SOURCES))
+        if _newer(lib, objs):
+            cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", lib] + objs + ["-lz", "-lpthread"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
     cli_src = os.path.join(CSRC, "cli.cpp")
     if os.path.exists(cli_src) and _newer(CLI, [cli_src, LIB, os.path.join(ROOT, "include", "ctb.h")]):
         cmd = [NVCC] + ARCH + COMMON + ["-o", CLI, cli_src, f"-L{HERE}", "-lctb", "-Xlinker", "-rpath,$ORIGIN"]

@@ -181,6 +181,29 @@ int ctb_diag_bounded_wait(int device, unsigned limit) {
 
 void ctb_diag_force_overflow(int every) { ctb::bp_force_overflow(every); }
 
+void ctb_diag_fail_allocation(long nth) { ctb::fail_allocation_after(nth); }
+
+int ctb_diag_bounds_status(int device, int* checked_build, unsigned* violations, unsigned long long* first,
+                           int reset) {
+    if (!checked_build || !violations || !first) return arg_error("null pointer");
+#ifdef CTB_BOUNDS_CHECK
+    *checked_build = 1;
+#else
+    *checked_build = 0;
+#endif
+    int prev = 0;
+    CTB_CUDA_TRY(cudaGetDevice(&prev));
+    CTB_CUDA_TRY(cudaSetDevice(device));
+    unsigned c1 = 0, c2 = 0;
+    unsigned long long f1 = 0, f2 = 0;
+    int st = ctb::bounds_status_tma(&c1, &f1, reset);
+    if (st == CTB_OK) st = ctb::bounds_status_gather(&c2, &f2, reset);
+    cudaSetDevice(prev);
+    *violations = c1 + c2;
+    *first = f1 ? f1 : f2;
+    return st;
+}
+
 int ctb_forward_project(const float* vol, const double* angles_deg, const double* height_offsets_px, int n_views,
                         const ctb_detector* det, const ctb_grid* grid, int z_begin, int z_end, float* proj,
                         int accumulate, void* stream) {
@@ -366,6 +389,36 @@ int ctb_get_cross_section(const ctb_ctx* ctx, int axis, int index, float* out, i
     if (axis < CTB_AXIS_X || axis > CTB_AXIS_Z) return arg_error("unknown axis");
     const int st = ctx->r.cross_section(axis, index, out, rows, cols);
     if (st != CTB_OK) ctb::set_global_error("no reconstructed volume or index out of bounds");
+    return st;
+}
+
+int ctb_forward(ctb_ctx* ctx, const float* host_volume, float* host_projections) {
+    if (!ctx) return arg_error("null context");
+    return ctx->r.forward(host_volume, host_projections);
+}
+
+int ctb_backward(ctb_ctx* ctx, const float* host_projections, float* host_volume) {
+    if (!ctx) return arg_error("null context");
+    return ctx->r.backward(host_projections, host_volume);
+}
+
+int ctb_gradient(ctb_ctx* ctx, const float* host_volume, const float* host_data, float* host_gradient,
+                 double* loss) {
+    if (!ctx) return arg_error("null context");
+    return ctx->r.gradient(host_volume, host_data, host_gradient, loss);
+}
+
+int ctb_batch_reconstruct(ctb_ctx* ctx, int n_scans, const ctb_scan* scans, void* stream) {
+    if (!ctx) return arg_error("null context");
+    ctb_batch* b = nullptr;
+    int st = ctb_batch_create(&b, n_scans, scans, ctx->r.precision(), stream);
+    if (st == CTB_OK) st = ctb_batch_run(b, stream);
+    if (b) {
+        // the graph reads the batch's buffers until it has run
+        const cudaError_t e = cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+        if (st == CTB_OK && e != cudaSuccess) st = ctb::cuda_status(e, "ctb_batch_reconstruct");
+        ctb_batch_destroy(b);
+    }
     return st;
 }
 

@@ -40,6 +40,10 @@ inline bool valid_grid(const ctb_grid* g) {
            g->y_from >= 0 && g->y_to > g->y_from && g->z_from >= 0 && g->z_to > g->z_from && g->voxel_pitch > 0;
 }
 
+// Diagnostic: the n-th device or host allocation of the facade from now on
+// fails as if memory were exhausted (0 = off).
+void fail_allocation_after(long n);
+
 inline size_t store_bytes(int store_type) { return store_type == CTB_FP32 ? 4 : 2; }
 inline size_t raw_bytes(int raw_type) { return raw_type == CTB_U8 ? 1 : raw_type == CTB_U16 ? 2 : 4; }
 
@@ -175,6 +179,11 @@ int bp_batch_launch(const BpBatchPlan& plan, const void* desc, const long long* 
 // `every` read their texels through global memory, as views whose footprint
 // exceeds the box do (0 = off). Results do not change.
 void bp_force_overflow(int every);
+// Bounds-checked build: out-of-range texel fetches recorded by the shared-memory
+// (TMA) and global-gather backprojectors since the last reset; always 0 in the
+// normal build.
+int bounds_status_tma(unsigned* count, unsigned long long* first, int reset);
+int bounds_status_gather(unsigned* count, unsigned long long* first, int reset);
 // Number of CTAs whose bounded mbarrier waits gave up since the last reset.
 int device_wait_timeouts(unsigned* count, int reset);
 // Run a wait that can never complete with the given try limit (diagnostic of
@@ -183,6 +192,8 @@ int bounded_wait_probe_run(unsigned limit, cudaStream_t s);
 
 int forward_launch(const float* vol, const float4* views, int n_views, const ProjGeom& g, float* proj,
                    int accumulate, cudaStream_t s);
+// r = a - b (n floats); adds the sum of r^2 to *sumsq (device double)
+int residual_launch(const float* a, const float* b, float* r, long long n, double* sumsq, cudaStream_t s);
 
 // ----------------------------------------------------------------- layout
 int layout_launch(const float* src, int x, int y, int zs, int index_order, int byte_order, void* dst,

@@ -22,6 +22,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <fstream>
 #include <sstream>
 #include <thread>
@@ -31,10 +32,29 @@
 namespace ctb {
 
 // ------------------------------------------------------------------ buffers
+// Diagnostic allocation failure (ctb_diag_fail_allocation): while positive,
+// every device or host allocation of the facade counts it down and the one
+// that brings it to zero fails as if the memory were exhausted.
+static std::atomic<long> g_fail_countdown{0};
+
+void fail_allocation_after(long n) { g_fail_countdown.store(n > 0 ? n : 0); }
+
+static bool injected_failure() {
+    long c = g_fail_countdown.load();
+    while (c > 0)
+        if (g_fail_countdown.compare_exchange_weak(c, c - 1)) return c == 1;
+    return false;
+}
+
 int DevBuf::ensure(size_t n, const char* what) {
     if (n <= bytes && p) return CTB_OK;
     release();
     if (n == 0) return CTB_OK;
+    if (injected_failure()) {
+        set_global_error(std::string("device allocation of ") + std::to_string(n >> 20) + " MB for " + what +
+                         " failed (injected)");
+        return CTB_ERR_ALLOC;
+    }
     cudaError_t e = cudaMalloc(&p, n);
     if (e != cudaSuccess) {
         p = nullptr;
@@ -56,6 +76,7 @@ int HostBuf::ensure(size_t n) {
     if (n <= bytes && p) return CTB_OK;
     release();
     if (n == 0) return CTB_OK;
+    if (injected_failure()) return CTB_ERR_ALLOC;
     if (cudaHostAlloc(&p, n, cudaHostAllocPortable) == cudaSuccess) {
         pinned = true;
     } else {

@@ -65,6 +65,16 @@ void gpu_weights_from(const int* sm_count, const double* bandwidth, int n, doubl
 // device also takes what rounding left over, so every slice is covered once.
 void split_slices(const double* weights, int n, int z, int* begin);
 
+// Device resources of the context's operator calls (forward, backward,
+// gradient) on its first active device.
+struct OpWork {
+    int device = -1;
+    cudaStream_t s = nullptr;
+    DevBuf d_proj, d_data, d_slab, d_views, d_angles, d_heights, d_sum;
+    explicit OpWork(int d) : device(d) {}
+    ~OpWork();
+};
+
 class Reconstructor {
    public:
     Reconstructor();
@@ -107,6 +117,7 @@ class Reconstructor {
     int views() const { return int(angles_.size()); }
     double pixel_size() const { return pixel_size_; }
     const ctb_timings& timings() const { return tm_; }
+    int precision() const { return store_; }
     void settings(ctb_settings* s) const;
     size_t required_memory() const;
     // getProjectionAt: angle, relative height offset (pixels) and, if image is
@@ -119,6 +130,13 @@ class Reconstructor {
     int cross_section(int axis, int index, float* out, int* rows, int* cols) const;
     int save(const std::string& path, int index_order, int byte_order);
     void stop() { stop_ = true; }
+
+    // ---- matched projector pair on the context's scan geometry and box
+    // (host X-fastest volume, host V x H x W float projections; slab by slab)
+    int forward(const float* host_vol, float* host_proj);
+    int backward(const float* host_proj, float* host_vol);
+    // f = ||A x - p||^2 and its gradient 2 A^T (A x - p)
+    int gradient(const float* host_vol, const float* host_data, float* host_grad, double* f);
 
     const std::string& error() const { return err_; }
 
@@ -183,6 +201,10 @@ class Reconstructor {
 
     // cached per-device resources, one entry per active device
     std::vector<std::unique_ptr<DeviceWork>> workers_;
+    std::unique_ptr<OpWork> op_;
+    int op_prepare(int* slab);
+    int op_forward(const float* host_vol, int slab);
+    int op_backward(const float* d_proj, float* host_vol, float scale, int slab);
     std::mutex progress_mtx_;
 };
 

@@ -86,15 +86,22 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ pro
             const float ui = __fadd_rn(u, g.uPre);
             const int u0 = int(ui);
             const float fu = __fsub_rn(ui, float(u0));
+#ifdef CTB_BOUNDS_CHECK
+            const T* col = pv + (CTB_FETCH_OK(u0, g.W - 1, 6) ? u0 : 0);
+#else
             const T* col = pv + u0;
+#endif
             const RowLine rl = row_line(U, q.z, g.zpv, g.vs, g.vPre);
 #pragma unroll
             for (int j = 0; j < ZC; ++j) {
                 const float vi = row_at(rl, float(g.z_begin + z0 + j));
                 const float zw = __fmul_rn(__fsub_rn(float(z0 + j), g.zPre), g.vs);
                 if (v_inside(zw, q.z, U, g.lbV, g.ubV)) {
-                    const int v0 = int(vi);
+                    int v0 = int(vi);
                     const float fv = __fsub_rn(vi, float(v0));
+#ifdef CTB_BOUNDS_CHECK
+                    if (!CTB_FETCH_OK(v0, g.H - 1, 7)) v0 = 0;
+#endif
                     const T* r0 = col + (long long)v0 * g.pitch;
                     const float a = (1.0f - fu) * ld(r0) + fu * ld(r0 + 1);
                     const float b = (1.0f - fu) * ld(r0 + g.pitch) + fu * ld(r0 + g.pitch + 1);
@@ -131,6 +138,24 @@ int bp_launch_typed(const T* proj, const float4* views, int n_views, const ProjG
 }
 
 }  // namespace
+
+int bounds_status_gather(unsigned* count, unsigned long long* first, int reset) {
+#ifdef CTB_BOUNDS_CHECK
+    CTB_CUDA_TRY(cudaMemcpyFromSymbol(count, g_bounds_count, sizeof(unsigned)));
+    CTB_CUDA_TRY(cudaMemcpyFromSymbol(first, g_bounds_first, sizeof(unsigned long long)));
+    if (reset) {
+        const unsigned z = 0;
+        const unsigned long long zz = 0;
+        CTB_CUDA_TRY(cudaMemcpyToSymbol(g_bounds_count, &z, sizeof z));
+        CTB_CUDA_TRY(cudaMemcpyToSymbol(g_bounds_first, &zz, sizeof zz));
+    }
+#else
+    (void)reset;
+    *count = 0;
+    *first = 0;
+#endif
+    return CTB_OK;
+}
 
 int view_table_build(const double* angles_deg_dev, const double* heights_dev, int n, float4* out,
                      cudaStream_t s) {

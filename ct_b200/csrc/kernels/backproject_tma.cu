@@ -91,9 +91,14 @@ template <> __device__ __forceinline__ float sval<__nv_bfloat16>(__nv_bfloat16 v
 // zero (exact for 0 <= vi < 2^22; the caller guarantees vi >= 0.5), whose low
 // bits are the row index and whose difference from the magic is float(v0);
 // subtractions are FMAs with a -1 factor (one rounding, as a subtraction).
+// Rows of the box relative to its origin row, for the bounds-checked build.
+struct BoxRows {
+    int oy, BV;
+};
+
 template <typename T, int ZC>
 __device__ __forceinline__ void column_pairs(const T* col, const int BU, const float* zf, float mdv, float c0,
-                                             float fu, float w, float* acc) {
+                                             float fu, float w, float* acc, BoxRows br) {
     constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
     const float2 mdv2 = make_float2(mdv, mdv), c02 = make_float2(c0, c0);
     const float2 fu2 = make_float2(fu, fu), w2 = make_float2(w, w);
@@ -104,8 +109,13 @@ __device__ __forceinline__ void column_pairs(const T* col, const int BU, const f
         const float2 sm = __fadd2_rz(vi, mg);
         const float2 nfl = __ffma2_rn(sm, m1, mg);   // -float(floor(vi))
         const float2 fv = __fadd2_rn(vi, nfl);
-        const T* ra = col + (__float_as_int(sm.x) - 0x4B400000) * BU;
-        const T* rb = col + (__float_as_int(sm.y) - 0x4B400000) * BU;
+        int rowa = __float_as_int(sm.x) - 0x4B400000, rowb = __float_as_int(sm.y) - 0x4B400000;
+#ifdef CTB_BOUNDS_CHECK
+        if (!CTB_FETCH_OK(rowa - br.oy, br.BV - 1, 1)) rowa = br.oy;
+        if (!CTB_FETCH_OK(rowb - br.oy, br.BV - 1, 1)) rowb = br.oy;
+#endif
+        const T* ra = col + rowa * BU;
+        const T* rb = col + rowb * BU;
         const float2 p00 = make_float2(sval(ra[0]), sval(rb[0])), p01 = make_float2(sval(ra[1]), sval(rb[1]));
         const float2 p10 = make_float2(sval(ra[BU]), sval(rb[BU])), p11 = make_float2(sval(ra[BU + 1]), sval(rb[BU + 1]));
         const float2 a = __ffma2_rn(fu2, __ffma2_rn(p00, m1, p01), p00);
@@ -305,13 +315,17 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                 const float vf = row_at(rl, zf[0]), vl = row_at(rl, zf[ZC - 1]);
                 if (!p.ovf[b]) {
                     const int2 o = p.org[b];
-                    const T* col = buf + size_t(b) * buf_stride + (u0 - o.x) - o.y * bx.BU;
+                    int cu = u0 - o.x;   // column of u0 in the box
+#ifdef CTB_BOUNDS_CHECK
+                    if (!CTB_FETCH_OK(cu, bx.BU - 1, 2)) cu = 0;
+#endif
+                    const T* col = buf + size_t(b) * buf_stride + cu - o.y * bx.BU;
                     const int BU = bx.BU;
                     // strictly inside the row bounds (half-pixel margin): every voxel of the column passes
                     // the per-voxel membership test, so this loop and the checked one take the same
                     // decisions
                     if (fminf(vf, vl) >= 0.5f && fmaxf(vf, vl) <= g.vi_hi - 0.5f) {
-                        column_pairs<T, ZC>(col, BU, zf, rl.mdv, rl.c0, fu, w, acc);
+                        column_pairs<T, ZC>(col, BU, zf, rl.mdv, rl.c0, fu, w, acc, BoxRows{o.y, bx.BV});
                     } else {
                         int ja, jb;
                         v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);
@@ -319,8 +333,11 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                         for (int j = 0; j < ZC; ++j) {
                             const float vi = row_at(rl, zf[j]);
                             if (j >= ja && j <= jb) {
-                                const int v0 = int(vi);
+                                int v0 = int(vi);
                                 const float fv = __fsub_rn(vi, float(v0));
+#ifdef CTB_BOUNDS_CHECK
+                                if (!CTB_FETCH_OK(v0 - o.y, bx.BV - 1, 1)) v0 = o.y;
+#endif
                                 const T* r0 = col + v0 * BU;
                                 const float p00 = sval(r0[0]), p01 = sval(r0[1]);
                                 const float p10 = sval(r0[BU]), p11 = sval(r0[BU + 1]);
@@ -332,15 +349,23 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                     }
                 } else {
                     // the view staged in this buffer (the tile's view order is rotated)
-                    const T* col = proj + (long long)p.vv[b] * g.view_stride + u0;
+                    int gv = p.vv[b], gu = u0;
+#ifdef CTB_BOUNDS_CHECK
+                    if (!CTB_FETCH_OK(gv, n_views, 5)) gv = 0;
+                    if (!CTB_FETCH_OK(gu, g.W - 1, 3)) gu = 0;
+#endif
+                    const T* col = proj + (long long)gv * g.view_stride + gu;
                     int ja, jb;
                     v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);
 #pragma unroll
                     for (int j = 0; j < ZC; ++j) {
                         const float vi = row_at(rl, zf[j]);
                         if (j >= ja && j <= jb) {
-                            const int v0 = int(vi);
+                            int v0 = int(vi);
                             const float fv = __fsub_rn(vi, float(v0));
+#ifdef CTB_BOUNDS_CHECK
+                            if (!CTB_FETCH_OK(v0, g.H - 1, 4)) v0 = 0;
+#endif
                             const T* r0 = col + (long long)v0 * g.pitch;
                             const float a = fmaf(fu, gval(r0 + 1) - gval(r0), gval(r0));
                             const float c = fmaf(fu, gval(r0 + g.pitch + 1) - gval(r0 + g.pitch), gval(r0 + g.pitch));
@@ -759,6 +784,24 @@ int bounded_wait_probe_run(unsigned limit, cudaStream_t s) {
 }
 
 void bp_force_overflow(int every) { g_ovf_every.store(every > 0 ? every : 0); }
+
+int bounds_status_tma(unsigned* count, unsigned long long* first, int reset) {
+#ifdef CTB_BOUNDS_CHECK
+    CTB_CUDA_TRY(cudaMemcpyFromSymbol(count, g_bounds_count, sizeof(unsigned)));
+    CTB_CUDA_TRY(cudaMemcpyFromSymbol(first, g_bounds_first, sizeof(unsigned long long)));
+    if (reset) {
+        const unsigned z = 0;
+        const unsigned long long zz = 0;
+        CTB_CUDA_TRY(cudaMemcpyToSymbol(g_bounds_count, &z, sizeof z));
+        CTB_CUDA_TRY(cudaMemcpyToSymbol(g_bounds_first, &zz, sizeof zz));
+    }
+#else
+    (void)reset;
+    *count = 0;
+    *first = 0;
+#endif
+    return CTB_OK;
+}
 
 int device_wait_timeouts(unsigned* count, int reset) {
     CTB_CUDA_TRY(cudaMemcpyFromSymbol(count, g_wait_timeouts, sizeof(unsigned)));

@@ -35,6 +35,8 @@
 // The volume is read in a z-fastest copy so that a warp's lanes (consecutive
 // rows -> consecutive z) read contiguous memory.
 
+#include <algorithm>
+
 #include "../ctb_internal.h"
 #include "geom.cuh"
 
@@ -239,6 +241,38 @@ int forward_launch(const float* vol, const float4* views, int n_views, const Pro
     }
     cudaFreeAsync(volz, s);
     return st;
+}
+
+namespace {
+// r = a - b over n values; the sum of r^2 is added to *sumsq (double)
+__global__ void residual_kernel(const float* __restrict__ a, const float* __restrict__ b, float* __restrict__ r,
+                                long long n, double* __restrict__ sumsq) {
+    double acc = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float d = a[i] - b[i];
+        r[i] = d;
+        acc += double(d) * double(d);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    __shared__ double part[8];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < int(blockDim.x >> 5); ++w) t += part[w];
+        atomicAdd(sumsq, t);
+    }
+}
+}  // namespace
+
+int residual_launch(const float* a, const float* b, float* r, long long n, double* sumsq, cudaStream_t s) {
+    if (n <= 0) return CTB_OK;
+    int dev = 0, sms = 0;
+    CTB_CUDA_TRY(cudaGetDevice(&dev));
+    CTB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long blocks = std::min<long long>((n + 255) / 256, 8LL * sms);
+    residual_kernel<<<int(blocks), 256, 0, s>>>(a, b, r, n, sumsq);
+    return cuda_status(cudaGetLastError(), "residual_kernel launch");
 }
 
 }  // namespace ctb

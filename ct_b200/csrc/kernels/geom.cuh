@@ -12,6 +12,27 @@
 
 namespace ctb {
 
+// Bounds-checked build (-DCTB_BOUNDS_CHECK, libctb_checked.so): every texel
+// fetch of the backprojectors is checked against the buffer it reads (the
+// staged box, or the projections in global memory) before it is made. A
+// fetch out of range is skipped (reads as 0) and recorded in this file's
+// status words: a count and the first offender (site << 56 | index). Nothing
+// traps. In the normal build the checks compile to nothing.
+#ifdef CTB_BOUNDS_CHECK
+static __device__ unsigned int g_bounds_count;
+static __device__ unsigned long long g_bounds_first;
+__device__ __forceinline__ bool fetch_ok(long long idx, long long lim, unsigned site) {
+    if (idx >= 0 && idx < lim) return true;
+    atomicAdd(&g_bounds_count, 1u);
+    atomicCAS(&g_bounds_first, 0ull,
+              (static_cast<unsigned long long>(site) << 56) | (static_cast<unsigned long long>(idx) & ((1ull << 56) - 1)));
+    return false;
+}
+#define CTB_FETCH_OK(idx, lim, site) ::ctb::fetch_ok((idx), (lim), (site))
+#else
+#define CTB_FETCH_OK(idx, lim, site) true
+#endif
+
 __device__ __forceinline__ float world_coord(int idx, float pre, float vs) {
     return __fmul_rn(__fsub_rn(float(idx), pre), vs);
 }

@@ -161,6 +161,35 @@ class CtVolume:
     def saveVolumeToBinaryFile(self, filename: str, indexOrder: int = L.Z_FASTEST, byteOrder: int = L.LITTLE_ENDIAN):
         self._ck(lib().ctb_save_volume(self._ctx, str(filename).encode(), indexOrder, byteOrder))
 
+    # ------------------------------------------------ matched projector pair (no reference counterpart)
+    def _proj_shape(self):
+        d = self.detector()
+        return (self.getSinogramSize(), d.height, d.width)
+
+    def forwardProject(self, volume: np.ndarray) -> np.ndarray:
+        """A x: the forward projector on this scan's views and box; volume (Z, Y, X) float32 -> (V, H, W)."""
+        x = np.ascontiguousarray(volume, np.float32)
+        out = np.empty(self._proj_shape(), np.float32)
+        self._ck(lib().ctb_forward(self._ctx, x.ctypes.data, out.ctypes.data))
+        return out
+
+    def backProject(self, projections: np.ndarray) -> np.ndarray:
+        """A^T y: the exact transpose of forwardProject (unfiltered); (V, H, W) float32 -> (Z, Y, X)."""
+        y = np.ascontiguousarray(projections, np.float32)
+        X, Y, Z = self.grid().box
+        out = np.empty((Z, Y, X), np.float32)
+        self._ck(lib().ctb_backward(self._ctx, y.ctypes.data, out.ctypes.data))
+        return out
+
+    def gradient(self, volume: np.ndarray, data: np.ndarray):
+        """(||A x - p||^2, 2 A^T (A x - p)) for volume x (Z, Y, X) and data p (V, H, W)."""
+        x = np.ascontiguousarray(volume, np.float32)
+        p = np.ascontiguousarray(data, np.float32)
+        g = np.empty_like(x)
+        f = ctypes.c_double()
+        self._ck(lib().ctb_gradient(self._ctx, x.ctypes.data, p.ctypes.data, g.ctypes.data, ctypes.byref(f)))
+        return f.value, g
+
     def getVolumeCrossSection(self, axis: int, index: int) -> np.ndarray:
         """Cross section of the last volume, left-handed orientation (Volume::getVolumeCrossSection)."""
         rows, cols = ctypes.c_int(), ctypes.c_int()

@@ -175,6 +175,24 @@ class Batch:
             self._h = None
 
 
+def batch_reconstruct(scans, store=L.FP32, stream=None):
+    """One-shot batch (ctb_batch_reconstruct on a context of the given
+    precision): create, run, synchronise and release. Same scan dicts as Batch."""
+    from .ctvolume import CtVolume
+    keep = []
+    arr = (L.Scan * len(scans))()
+    for i, sc in enumerate(scans):
+        a = np.ascontiguousarray(sc["angles_deg"], np.float64)
+        h = None if sc.get("heights_px") is None else np.ascontiguousarray(sc["heights_px"], np.float64)
+        keep += [a, h]
+        arr[i] = L.Scan(ctypes.c_void_p(sc["raw"].data_ptr()), RAW_CODES_FN()[sc["raw"].dtype], len(a),
+                        a.ctypes.data, None if h is None else h.ctypes.data, sc["det"], sc["grid"],
+                        sc.get("filter", L.RAMLAK), sc.get("pad", 1), ctypes.c_void_p(sc["vol"].data_ptr()))
+    ctx = CtVolume()
+    ctx.setPrecision(store)
+    ctx._ck(lib().ctb_batch_reconstruct(ctx._ctx, len(scans), arr, _stream(stream)))
+
+
 def RAW_CODES_FN():
     _torch()
     return RAW_CODES

@@ -190,6 +190,7 @@ typedef struct {
 } ctb_scan;
 
 typedef struct ctb_batch ctb_batch;
+typedef struct ctb_ctx ctb_ctx;   /* reconstruction context (facade layer below) */
 
 /* Many independent scans of different detector, view and volume sizes
  * reconstructed together: per-scan filtering followed by ONE persistent
@@ -209,10 +210,14 @@ int ctb_batch_run_sequential(ctb_batch* batch, void* stream);  /* scan by scan, 
 int ctb_batch_tuning(const ctb_batch* batch, int* zc, double* ms_zc32, double* ms_zc16, double* ms_zc8,
                      int* n_persistent);
 void ctb_batch_destroy(ctb_batch* batch);
+/* One call for a batch on a context: ctb_batch_create with the context's
+ * precision (ctb_set_precision), ctb_batch_run, a synchronisation of the
+ * stream and ctb_batch_destroy. For repeated batches of the same scans keep
+ * a ctb_batch instead (the tuning and the graph capture are done once). */
+int ctb_batch_reconstruct(ctb_ctx* ctx, int n_scans, const ctb_scan* scans, void* stream);
 
 /* ------------------------------------------------------ facade layer */
 
-typedef struct ctb_ctx ctb_ctx;
 
 /* Progress callback: stage 0 = loading, 1 = reconstruction, 2 = saving;
  * percent 0..100 (Ct/CtVolume.h:271-276 signals). Fires on the calling thread. */
@@ -304,6 +309,23 @@ int ctb_get_volume(const ctb_ctx* ctx, float* host_volume, int index_order);
  * <base>.vgi header, raw float32 in index_order / byte_order. */
 int ctb_save_volume(ctb_ctx* ctx, const char* path, int index_order, int byte_order);
 
+/* The matched projector pair on the context's scan (detector, views, height
+ * offsets, all views regardless of the skip setting) and box (grid and
+ * bounds), host memory in and out, on the first active device; the volume
+ * moves through the device one z-slab at a time, nothing else is kept.
+ * Volumes are X-fastest box volumes (x*y*z floats), projections n_views x H x
+ * W floats. No counterpart in the reference (which has no forward model).
+ *   ctb_forward:  projections = A volume (the forward projector, fp_kernel)
+ *   ctb_backward: volume = A^T projections (the backprojector, load scale 1,
+ *                 unfiltered: the exact transpose of A)
+ *   ctb_gradient: loss = ||A volume - data||^2 and gradient = 2 A^T (A volume
+ *                 - data), with A volume accumulated slab by slab and the
+ *                 adjoint recomputed per slab (no stored intermediates). */
+int ctb_forward(ctb_ctx* ctx, const float* host_volume, float* host_projections);
+int ctb_backward(ctb_ctx* ctx, const float* host_projections, float* host_volume);
+int ctb_gradient(ctb_ctx* ctx, const float* host_volume, const float* host_data, float* host_gradient,
+                 double* loss);
+
 /* stop() (Ct/CtVolume.cpp:723-726): thread-safe, polled per slab / view group. */
 void ctb_stop(ctb_ctx* ctx);
 
@@ -369,6 +391,24 @@ int ctb_diag_bounded_wait(int device, unsigned limit);
  * views whose footprint does not fit the staged box. The result must not
  * change; 0 turns it off. Process-wide. No reference counterpart. */
 void ctb_diag_force_overflow(int every);
+
+/* Diagnostic of the facade's allocation failure path: from now on the nth
+ * device or host buffer the facade allocates (1 = the next one) fails as if
+ * the memory were exhausted, so ctb_reconstruct* returns CTB_ERR_ALLOC (the
+ * reference's VRAM / RAM failure branches, Ct/CtVolume.cpp:554-557,
+ * :1133-1147). 0 turns it off. Process-wide; no GPU fault is involved. */
+void ctb_diag_fail_allocation(long nth);
+
+/* Bounds-checked build (libctb_checked.so, compiled with CTB_BOUNDS_CHECK):
+ * the backprojection kernels check every texel fetch against the buffer it
+ * reads (the staged box in shared memory, or the projections in global
+ * memory), skip a fetch out of range and record it: *violations counts them
+ * on `device` since the last reset and *first encodes the first one
+ * (site << 56 | index). *checked_build is 0 in the normal library, whose
+ * kernels carry no checks (the counts are then 0). reset != 0 clears them.
+ * No reference counterpart (compute-sanitizer's memcheck is not used). */
+int ctb_diag_bounds_status(int device, int* checked_build, unsigned* violations, unsigned long long* first,
+                           int reset);
 
 /* ------------------------------------------------------ projection images */
 

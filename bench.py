@@ -452,18 +452,23 @@ def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
     Aty = ops.backproject(y, ang, None, d, grid)
     lhs, rhs = float((Ax.double() * y.double()).sum()), float((x.double() * Aty.double()).sum())
     out["dot_test_rel"] = abs(lhs - rhs) / max(abs(lhs), abs(rhs))
-    # device time of one A and one A^T (CUDA events, after the warm-up above)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    reps = 3
-    ev[0].record()
-    for _ in range(reps):
-        ops.forward_project(x, ang, None, d, grid, out=Ax)
-    ev[1].record()
-    for _ in range(reps):
-        ops.backproject(y, ang, None, d, grid, out=Aty)
-    ev[2].record()
-    torch.cuda.synchronize()
-    fp_ms, bp_ms = ev[0].elapsed_time(ev[1]) / reps, ev[1].elapsed_time(ev[2]) / reps
+    # device time of one A and one A^T (CUDA events around each call, after the warm-up
+    # above; the median of five)
+    def per_call(fn, reps=5):
+        ts = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts)), float(np.min(ts)), float(np.max(ts))
+
+    fp_ms, fp_min, fp_max = per_call(lambda: ops.forward_project(x, ang, None, d, grid, out=Ax))
+    bp_ms, bp_min, bp_max = per_call(lambda: ops.backproject(y, ang, None, d, grid, out=Aty))
+    out["forward_ms_min_max"] = [fp_min, fp_max]
+    out["backproject_ms_min_max"] = [bp_min, bp_max]
     out.update({"forward_ms": fp_ms, "forward_gups": units / fp_ms / 1e6,
                 "backproject_fp32_ms": bp_ms, "backproject_fp32_gups": units / bp_ms / 1e6})
     del Ax, Aty, y, x
@@ -538,6 +543,42 @@ def gradient_c4(edge=512, views=360, det=512, iters=20, seed=4):
     del p, truth, scan, fdk
     torch.cuda.empty_cache()
     return out
+
+
+def facade_split(v, host_out, n, V, W, H, Z, Y, X, units, edge, vs, det, geom, reps=2):
+    """One scan through the facade with the active device list [0] * n (the reference's launchCudaThreads
+    z split, Ct/CtVolume.cpp:1322-1351): per-worker slices and detector row bands, bytes copied, seconds,
+    and the largest difference from the one-device volume already in host_out."""
+    import torch
+
+    from ct_b200 import ops
+    from ct_b200 import _lib as L
+    one = host_out.clone()
+    v.setActiveCudaDevices([0] * n)
+    weights = np.full(n, 1.0 / n)
+    begin = np.zeros(n + 1, np.int32)
+    L.lib().ctb_split_slices(weights.ctypes.data, n, Z, begin.ctypes.data)
+    grid = v.grid()
+    workers = []
+    for i in range(n):
+        r_lo, rows = ops.row_band(v.detector(), grid, int(begin[i]), int(begin[i + 1]))
+        workers.append({"slices": [int(begin[i]), int(begin[i + 1])], "detector_rows": [r_lo, r_lo + rows]})
+    v.reconstructInto(host_out.data_ptr(), L.X_FASTEST)  # warm-up of the new workers
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        v.reconstructInto(host_out.data_ptr(), L.X_FASTEST)
+        ts.append(time.perf_counter() - t0)
+    tm = v.timings()
+    diff = float((host_out - one).abs().max())
+    scale = float(one.abs().max())
+    v.setActiveCudaDevices([0])
+    del one
+    return {"devices": [0] * n, "workers": workers, "seconds": float(np.mean(ts)),
+            "gups": units / float(np.mean(ts)) / 1e9, "h2d_bytes": int(tm.h2d_bytes),
+            "d2h_bytes": int(tm.d2h_bytes), "max_abs_diff_vs_one_device": diff, "volume_max_abs": scale,
+            "note": "workers share one GPU here (device 0 listed twice): no speed-up is expected; on n GPUs each "
+                    "moves only its detector row band"}
 
 
 def workload_config(args, world):
@@ -671,7 +712,9 @@ def run_ours(args):
         v.setFrequencyFilterType(cfg["filter"])
         v.setPrecision(args.store)
         if args.e2e_slab > 0:
-            v.setSlabHeight(args.e2e_slab)   # else the facade's own choice (128 slices for 1024^3)
+            v.setSlabHeight(args.e2e_slab)   # else the facade's own (or the autotuner's) choice
+        else:
+            v.setAutotune(True)              # the first warm-up reconstruction tunes the backprojection
         for _ in range(args.warmup):
             v.reconstructInto(host_out.data_ptr(), L.X_FASTEST)
         barrier(world)
@@ -686,7 +729,14 @@ def run_ours(args):
         e2e = {"value": whole_job_gups(units, world, sec * 1e3), "unit": "GUPS", "seconds": sec,
                "h2d_bytes_per_step": int(tm.h2d_bytes), "d2h_bytes_per_step": int(tm.d2h_bytes),
                "stages_s": {"upload_exposed": tm.upload_s, "filter": tm.filter_s, "backproject": tm.backproject_s,
-                            "download_exposed": tm.download_s}}
+                            "download_exposed": tm.download_s},
+               "autotune": v.getTuning()}
+        # the facade's z split across devices (setActiveCudaDevices): device 0 listed
+        # args.split times, each worker reconstructing its run of slices from the
+        # detector rows those slices reach; compared with the one-device volume
+        if args.split > 1 and rank == 0 and world == 1:
+            e2e["split"] = facade_split(v, host_out, args.split, V, W, H, Z, Y, X, units, edge, vs, det, geom)
+            log(f"split: {e2e['split']}")
         del v, host_in, host_out
         log(f"e2e: {e2e}")
 
@@ -836,6 +886,8 @@ def main():
     ap.add_argument("--skip-accuracy", action="store_true")
     ap.add_argument("--skip-batch", action="store_true")
     ap.add_argument("--skip-c2", action="store_true")
+    ap.add_argument("--split", type=int, default=2,
+                    help="end-to-end leg: also run the facade's z split over device 0 listed this many times (0: off)")
     ap.add_argument("--skip-gradient", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":

@@ -62,6 +62,11 @@ class Timings(ctypes.Structure):
                 ("h2d_bytes", ctypes.c_double), ("d2h_bytes", ctypes.c_double)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("slab_slices", ctypes.c_int), ("zc", ctypes.c_int), ("views_in_flight", ctypes.c_int),
+                ("backproject_ms", ctypes.c_double), ("tuned", ctypes.c_int)]
+
+
 PROGRESS_CB = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_double, ctypes.c_void_p)
 PREVIEW_CB = ctypes.CFUNCTYPE(None, ctypes.c_double, ctypes.POINTER(ctypes.c_float), ctypes.c_int, ctypes.c_int,
                               ctypes.c_void_p)
@@ -85,6 +90,10 @@ SIGNATURES = {
     "ctb_backward": (I, [P, P, P]),
     "ctb_gradient": (I, [P, P, P, P, P]),
     "ctb_batch_reconstruct": (I, [P, I, P, P]),
+    "ctb_batch_tuning_detail": (I, [P, I, P, P, P, P]),
+    "ctb_set_autotune": (I, [P, I]),
+    "ctb_autotune": (I, [P, P]),
+    "ctb_get_tuning": (I, [P, P]),
     "ctb_convert_layout": (I, [P, I, I, I, I, I, P, P]),
     "ctb_create": (I, [P]),
     "ctb_destroy": (None, [P]),

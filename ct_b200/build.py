@@ -44,6 +44,7 @@ SOURCES = [
     "host/batch.cpp",
     "host/volume_reader.cpp",
     "host/operators.cpp",
+    "host/tuning.cpp",
     "capi.cpp",
     "noalloc.cu",
 ]

@@ -392,6 +392,22 @@ int ctb_get_cross_section(const ctb_ctx* ctx, int axis, int index, float* out, i
     return st;
 }
 
+int ctb_set_autotune(ctb_ctx* ctx, int on) {
+    if (!ctx) return arg_error("null context");
+    ctx->r.set_autotune(on != 0);
+    return CTB_OK;
+}
+
+int ctb_autotune(ctb_ctx* ctx, ctb_tuning* out) {
+    if (!ctx) return arg_error("null context");
+    return ctx->r.autotune(out);
+}
+
+int ctb_get_tuning(const ctb_ctx* ctx, ctb_tuning* out) {
+    if (!ctx || !out) return arg_error("null pointer");
+    return ctx->r.tuning(out);
+}
+
 int ctb_forward(ctb_ctx* ctx, const float* host_volume, float* host_projections) {
     if (!ctx) return arg_error("null context");
     return ctx->r.forward(host_volume, host_projections);

@@ -138,15 +138,21 @@ void row_band(const ctb_detector& det, const ctb_grid& grid, int z_begin, int z_
 // hmax bounds |height offset| (pixels) over the views. Dispatches to the
 // shared-memory (TMA) kernel when possible, else to the global-gather kernel.
 int bp_pick_zc(int slab_slices);
+// Launch shape of the shared-memory backprojector; 0 = the built-in choice.
+struct BpConfig {
+    int zc = 0;     // z voxels per thread (8, 16 or 32): the block tile's height
+    int nbuf = 0;   // projection boxes staged per CTA (2, 3 or 4): views in flight
+};
 int backproject_launch(const void* proj, int store_type, const float4* views, int n_views,
-                       const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s);
+                       const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s,
+                       BpConfig cfg = BpConfig());
 int backproject_global_launch(const void* proj, int store_type, const float4* views, int n_views,
                               const ProjGeom& g, float* vol, int accumulate, cudaStream_t s);
 // Returns CTB_ERR_UNSUPPORTED (nothing launched) when the geometry or layout
 // does not suit the TMA kernel. zc: z voxels per thread (8, 16 or 32).
 int backproject_tma_launch(const void* proj, int store_type, const float4* views, int n_views,
                            const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s,
-                           int zc = 16);
+                           int zc = 16, int nbuf = 0);
 
 // Persistent multi-scan backprojection: one launch takes (scan, tile) work
 // items from a device counter until every scan of the batch is done.
@@ -170,7 +176,7 @@ struct BpBatchPlan {
 };
 // Builds descriptors (tensor maps, boxes, tile counts) and launch shape for
 // every scan that suits the shared-memory kernel; lists the others.
-int bp_batch_plan(int store_type, int zc, const BpBatchScan* scans, int n, BpBatchPlan* plan);
+int bp_batch_plan(int store_type, int zc, const BpBatchScan* scans, int n, BpBatchPlan* plan, int nbuf = 0);
 // desc / tile_start: device copies of plan.desc / plan.tile_start; queue: a
 // device counter that must be zero at launch.
 int bp_batch_launch(const BpBatchPlan& plan, const void* desc, const long long* tile_start, int n,

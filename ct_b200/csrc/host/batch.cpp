@@ -28,8 +28,10 @@ struct ctb_batch {
     unsigned long long* d_queue = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int zc = 16;
-    double ms32 = -1, ms16 = -1, ms8 = -1;
+    int zc = 16, nbuf = 0;
+    double ms32 = -1, ms16 = -1, ms8 = -1;   // best time per z voxels per thread
+    std::vector<int> cand_zc, cand_nbuf;     // every timed candidate
+    std::vector<double> cand_ms;
 
     ~ctb_batch() {
         cudaSetDevice(device);
@@ -182,7 +184,8 @@ int ctb_batch_create(ctb_batch** out, int n, const ctb_scan* scans, int store_ty
         cudaGetLastError();
         return bail(fail("ctb_batch_create: out of device memory", CTB_ERR_ALLOC));
     }
-    // autotuner: z voxels per thread of the persistent kernel, timed on this batch
+    // autotuner: the persistent kernel's block tile height (z voxels per thread)
+    // and views in flight (projection boxes staged per CTA), timed on this batch
     std::string key = "batch:" + std::to_string(store_type) + ":" + std::to_string(n);
     for (const ctb_scan& sc : b->scans)
         key += ":" + std::to_string(sc.det.width) + "x" + std::to_string(sc.det.height) + "x" +
@@ -190,11 +193,14 @@ int ctb_batch_create(ctb_batch** out, int n, const ctb_scan* scans, int store_ty
                std::to_string(sc.grid.y_to - sc.grid.y_from) + "x" + std::to_string(sc.grid.z_to - sc.grid.z_from);
     std::vector<double> times;
     int plan_err = CTB_OK;
-    b->zc = Autotuner::instance().pick(
-        key, {32, 16, 8},
-        [&](int zc) -> double {
+    // candidates zc * 10 + boxes in flight (0: the built-in choice for the box size)
+    const std::vector<int> cands = {320, 322, 324, 160, 162, 164, 80};
+    const int choice = Autotuner::instance().pick(
+        key, cands,
+        [&](int c) -> double {
+            const int zc = c / 10, nb = c % 10;
             BpBatchPlan plan;
-            if (bp_batch_plan(store_type, zc, b->bp.data(), n, &plan) != CTB_OK) return -1.0;
+            if (bp_batch_plan(store_type, zc, b->bp.data(), n, &plan, nb) != CTB_OK) return -1.0;
             b->plan = plan;
             if (upload_plan(b, s) != CTB_OK) return -1.0;
             cudaEvent_t e0, e1;
@@ -213,8 +219,17 @@ int ctb_batch_create(ctb_batch** out, int n, const ctb_scan* scans, int store_ty
             return st == CTB_OK ? double(ms) : -1.0;
         },
         &times);
-    if (times.size() == 3) { b->ms32 = times[0]; b->ms16 = times[1]; b->ms8 = times[2]; }
-    int st = bp_batch_plan(store_type, b->zc, b->bp.data(), n, &b->plan);
+    b->zc = choice / 10;
+    b->nbuf = choice % 10;
+    for (size_t i = 0; i < times.size() && i < cands.size(); ++i) {
+        const int zc = cands[i] / 10;
+        b->cand_zc.push_back(zc);
+        b->cand_nbuf.push_back(cands[i] % 10);
+        b->cand_ms.push_back(times[i]);
+        double& best = zc == 32 ? b->ms32 : zc == 16 ? b->ms16 : b->ms8;
+        if (times[i] >= 0 && (best < 0 || times[i] < best)) best = times[i];
+    }
+    int st = bp_batch_plan(store_type, b->zc, b->bp.data(), n, &b->plan, b->nbuf);
     if (st != CTB_OK)
         return bail(fail("ctb_batch_create: a scan does not suit the persistent backprojector", plan_err ? plan_err : st));
     st = upload_plan(b, s);
@@ -268,6 +283,18 @@ int ctb_batch_tuning(const ctb_batch* b, int* zc, double* ms32, double* ms16, do
     if (ms16) *ms16 = b->ms16;
     if (ms8) *ms8 = b->ms8;
     if (n_persistent) *n_persistent = int(b->plan.included.size());
+    return CTB_OK;
+}
+
+int ctb_batch_tuning_detail(const ctb_batch* b, int max, int* zc, int* views_in_flight, double* ms, int* n) {
+    if (!b || !n) return ctb::fail("ctb_batch_tuning_detail: invalid arguments", CTB_ERR_ARG);
+    const int k = int(b->cand_ms.size());
+    *n = k;
+    for (int i = 0; i < k && i < max; ++i) {
+        if (zc) zc[i] = b->cand_zc[i];
+        if (views_in_flight) views_in_flight[i] = b->cand_nbuf[i];
+        if (ms) ms[i] = b->cand_ms[i];
+    }
     return CTB_OK;
 }
 

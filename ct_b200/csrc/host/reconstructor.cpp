@@ -629,6 +629,13 @@ int Reconstructor::reconstruct(float* host_out, int index_order) {
         }
     }
 
+    // the first reconstruction of a shape tunes the backprojection when asked
+    // to (single device; a failed tuning leaves the built-in choices)
+    if (autotune_on_ && devices_.size() == 1) {
+        ctb_tuning t;
+        if (autotune_locked(&t) != CTB_OK) err_.clear();
+    }
+
     // one worker per active device entry; workers keep their buffers while
     // the device list stays the same
     const int n = int(devices_.size());
@@ -803,7 +810,11 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
     // views of 2048^2 into 1024^3, end to end: 256 slices 0.6 % faster than
     // 128, fewer launch tails, while two slabs still cover the upload and the
     // cut last slab keeps the final download short)
-    int slab = slab_req_ > 0 ? slab_req_ : std::max(16, ((Zw + 3) / 4 + 15) / 16 * 16);
+    // the autotuner's choice for this shape when there is one (host/tuning.cpp)
+    BpConfig bpc;
+    int tuned_slab = 0;
+    const bool tuned = tuned_for(z_lo, z_hi, &bpc, &tuned_slab);
+    int slab = slab_req_ > 0 ? slab_req_ : tuned ? tuned_slab : std::max(16, ((Zw + 3) / 4 + 15) / 16 * 16);
     slab = std::min(slab, Zw);
     const bool convert = order == CTB_Z_FASTEST;
     {
@@ -961,7 +972,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
                 cudaEventRecord(tb[2 * nb_ev], w.s_comp);
                 if (backproject_launch((const char*)w.d_filtered.p + size_t(bp_from) * view_filt, store_,
                                        (const float4*)w.d_views.p + bp_from, c0 + n - bp_from, gpre[p], hmax,
-                                       (float*)w.d_slab[p].p, bp_from > 0, w.s_comp))
+                                       (float*)w.d_slab[p].p, bp_from > 0, w.s_comp, bpc))
                     return cuda_fail("backprojection launch");
                 cudaEventRecord(tb[2 * nb_ev + 1], w.s_comp);
                 ++nb_ev;
@@ -1002,7 +1013,7 @@ int Reconstructor::run_pipeline(DeviceWork& w, float* out, int order, int z_lo, 
             const ProjGeom g = slab_geom(zb, ze);
             cudaEventRecord(tb[2 * nb_ev], w.s_comp);
             if (backproject_launch(w.d_filtered.p, store_, (const float4*)w.d_views.p, V, g, hmax,
-                                   (float*)w.d_slab[b].p, 0, w.s_comp))
+                                   (float*)w.d_slab[b].p, 0, w.s_comp, bpc))
                 return cuda_fail("backprojection launch");
             cudaEventRecord(tb[2 * nb_ev + 1], w.s_comp);
             ++nb_ev;

@@ -131,6 +131,12 @@ class Reconstructor {
     int save(const std::string& path, int index_order, int byte_order);
     void stop() { stop_ = true; }
 
+    // ---- autotuner of the backprojection launch shape and slab height
+    // (host/tuning.cpp): tunes on the context's scan, remembered per shape
+    void set_autotune(bool on) { autotune_on_ = on; }
+    int autotune(ctb_tuning* out);
+    int tuning(ctb_tuning* out) const;
+
     // ---- matched projector pair on the context's scan geometry and box
     // (host X-fastest volume, host V x H x W float projections; slab by slab)
     int forward(const float* host_vol, float* host_proj);
@@ -202,6 +208,10 @@ class Reconstructor {
     // cached per-device resources, one entry per active device
     std::vector<std::unique_ptr<DeviceWork>> workers_;
     std::unique_ptr<OpWork> op_;
+    bool autotune_on_ = false;
+    int autotune_locked(ctb_tuning* out);
+    std::string tune_key(int z_lo, int z_hi) const;
+    bool tuned_for(int z_lo, int z_hi, BpConfig* cfg, int* slab) const;
     int op_prepare(int* slab);
     int op_forward(const float* host_vol, int slab);
     int op_backward(const float* d_proj, float* host_vol, float scale, int slab);

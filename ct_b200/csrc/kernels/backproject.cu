@@ -212,7 +212,7 @@ int bp_pick_zc(int Zs) {
 }
 
 int backproject_launch(const void* proj, int store_type, const float4* views, int n_views,
-                       const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s) {
+                       const ProjGeom& g, double hmax, float* vol, int accumulate, cudaStream_t s, BpConfig cfg) {
     // shared-memory staged kernel when the footprint bound and the 16-byte TMA
     // stride rule allow it; the global-gather kernel otherwise.
     // CTB_BP_VARIANT=global|tma forces one of them (tma fails when ineligible).
@@ -230,8 +230,8 @@ int backproject_launch(const void* proj, int store_type, const float4* views, in
         return (v == 8 || v == 16 || v == 32) ? v : 0;
     }();
     if (variant != 1) {
-        const int zc = zc_env ? zc_env : bp_pick_zc(g.Zs);
-        int st = backproject_tma_launch(proj, store_type, views, n_views, g, hmax, vol, accumulate, s, zc);
+        const int zc = zc_env ? zc_env : cfg.zc ? cfg.zc : bp_pick_zc(g.Zs);
+        int st = backproject_tma_launch(proj, store_type, views, n_views, g, hmax, vol, accumulate, s, zc, cfg.nbuf);
         // a taller tile's footprint may exceed the box limits where a shorter one fits
         if (st == CTB_ERR_UNSUPPORTED && !zc_env && zc > 16)
             st = backproject_tma_launch(proj, store_type, views, n_views, g, hmax, vol, accumulate, s, 16);

@@ -110,6 +110,21 @@ class CtVolume:
     def setSlabHeight(self, slices: int):
         self._ck(lib().ctb_set_slab_height(self._ctx, slices))
 
+    def setAutotune(self, on: bool):
+        """Tune the backprojection on the first reconstruction of each scan/box shape (ctb_set_autotune)."""
+        self._ck(lib().ctb_set_autotune(self._ctx, int(bool(on))))
+
+    def autotune(self) -> dict:
+        """Tune now on the loaded scan and box (ctb_autotune); the choice is kept for this shape."""
+        t = L.Tuning()
+        self._ck(lib().ctb_autotune(self._ctx, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in L.Tuning._fields_}
+
+    def getTuning(self) -> dict:
+        t = L.Tuning()
+        self._ck(lib().ctb_get_tuning(self._ctx, ctypes.byref(t)))
+        return {k: getattr(t, k) for k, _ in L.Tuning._fields_}
+
     def setProgressCallback(self, fn):
         """fn(stage, percent); stage 0 loading, 1 reconstruction, 2 saving."""
         self._cb = L.PROGRESS_CB(lambda s, p, u: fn(s, p)) if fn else L.PROGRESS_CB()

@@ -168,6 +168,16 @@ class Batch:
         return {"zc": zc.value, "ms_zc32": t32.value, "ms_zc16": t16.value, "ms_zc8": t8.value,
                 "persistent_scans": n.value}
 
+    def tuning_detail(self):
+        """Every candidate the autotuner timed: [(z voxels per thread, views in flight (0: built-in), ms)]."""
+        n = ctypes.c_int()
+        check(lib().ctb_batch_tuning_detail(self._h, 0, None, None, None, ctypes.byref(n)))
+        zc = (ctypes.c_int * n.value)()
+        nb = (ctypes.c_int * n.value)()
+        ms = (ctypes.c_double * n.value)()
+        check(lib().ctb_batch_tuning_detail(self._h, n.value, zc, nb, ms, ctypes.byref(n)))
+        return [(zc[i], nb[i], ms[i]) for i in range(n.value)]
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value and L._lib is not None:

@@ -209,6 +209,10 @@ int ctb_batch_run_sequential(ctb_batch* batch, void* stream);  /* scan by scan, 
  * budget get their own launch inside the same graph). */
 int ctb_batch_tuning(const ctb_batch* batch, int* zc, double* ms_zc32, double* ms_zc16, double* ms_zc8,
                      int* n_persistent);
+/* Every candidate the batch autotuner timed: z voxels per thread, views in
+ * flight (projection boxes staged per CTA; 0 = the built-in choice) and ms;
+ * *n receives the count, at most max entries are written. */
+int ctb_batch_tuning_detail(const ctb_batch* batch, int max, int* zc, int* views_in_flight, double* ms, int* n);
 void ctb_batch_destroy(ctb_batch* batch);
 /* One call for a batch on a context: ctb_batch_create with the context's
  * precision (ctb_set_precision), ctb_batch_run, a synchronisation of the
@@ -276,6 +280,27 @@ int ctb_set_pad(ctb_ctx* ctx, int pad);                   /* 1 (reference) or 2 
  * reference grid. */
 int ctb_set_grid(ctb_ctx* ctx, int x_size, int y_size, int z_size, float voxel_pitch);
 int ctb_set_slab_height(ctb_ctx* ctx, int slices);        /* 0 = automatic */
+
+/* Autotuner of the backprojection (no reference counterpart; the reference
+ * sizes its z-chunks by free memory only, getMaxChunkSize,
+ * Ct/CtVolume.cpp:1385-1397). ctb_autotune times, on the loaded scan and box
+ * and the first active device, the block tile height (z voxels per thread),
+ * the views in flight (projection boxes staged per CTA) and the slab height
+ * over an evenly spaced subset of the views, and keeps the fastest for every
+ * later reconstruction of the same scan/box shape in this process (single
+ * device; with several devices the built-in choices apply). With
+ * ctb_set_autotune(ctx, 1) the first reconstruction of each shape tunes by
+ * itself. 0 in a field means the built-in choice. */
+typedef struct {
+    int slab_slices;        /* z slices per backprojection launch */
+    int zc;                 /* z voxels per thread */
+    int views_in_flight;    /* projection boxes staged per CTA */
+    double backproject_ms;  /* tuned device time of the whole backprojection (estimated from the subset) */
+    int tuned;              /* 1 if a tuning exists for the context's current shape */
+} ctb_tuning;
+int ctb_set_autotune(ctb_ctx* ctx, int on);
+int ctb_autotune(ctb_ctx* ctx, ctb_tuning* out);
+int ctb_get_tuning(const ctb_ctx* ctx, ctb_tuning* out);
 int ctb_set_progress_callback(ctb_ctx* ctx, ctb_progress_cb cb, void* user);
 
 /* setUseCuda (Ct/CtVolume.h:104): 0 is refused (CTB_ERR_UNSUPPORTED), the

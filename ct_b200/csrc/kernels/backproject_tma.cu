@@ -569,18 +569,19 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     const double zabs =
         std::max(std::fabs((0 - g.zPre) * vs), std::fabs((g.Zs + ZC - 1 - g.zPre) * vs)) + hmax;
     const double vext = (ZC - 1) * vs * Umax + zabs * dU * T;
-    // Row stride: 64 bytes more than a multiple of 128, so two adjacent box
-    // rows sit 16 banks apart and a warp whose lanes sample one row pair
-    // within 16 banks' width never conflicts (1440 views of 2048^2 into
-    // 1024^3, box 96 / 112 texels wide: FP16 1 % faster than an odd number of
-    // 16-byte chunks, FP32 7 %).
-    // Strides past 256 texels fall back to the odd-chunk rule (consecutive
-    // rows start in different banks) to keep the box small.
-    const int chunk = 16 / esize, per128 = 128 / esize, half = 64 / esize;
+    // Row stride: 32 bytes more than a multiple of 128, so adjacent box rows
+    // sit 8 banks apart and only rows four apart in one column share a bank;
+    // the lanes of a warp (an 8 x 4 patch of columns) sample a few rows within
+    // a few words of each other, so they rarely do. 1440 views of 2048^2 into
+    // 1024^3 (boxes 80 texels wide, 72 for FP32): 2 % faster than 64 bytes past a multiple
+    // of 128 for 16-bit texels, 1 % for FP32, 5-8 % faster than an odd number
+    // of 16-byte chunks. Strides past 256 texels fall back to the odd-chunk
+    // rule (consecutive rows start in different banks) to keep the box small.
+    const int chunk = 16 / esize, per128 = 128 / esize, off = 32 / esize;
     int BU = int(std::ceil(uext)) + 12;
-    const int bu64 = (BU - half + per128 - 1) / per128 * per128 + half;
-    if (bu64 <= 256) {
-        BU = bu64;
+    const int bu32 = (BU - off + per128 - 1) / per128 * per128 + off;
+    if (bu32 <= 256) {
+        BU = bu32;
     } else {
         BU = (BU + chunk - 1) / chunk * chunk;
         if ((BU / chunk) % 2 == 0) BU += chunk;

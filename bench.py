@@ -43,11 +43,11 @@ CONFIGS = {
 FILTERS = {"ramlak": 0, "shepplogan": 1, "hann": 2}
 
 # DRAM bytes (read + write) of one backprojection launch per voxel-view update, from
-# ncu captures (dram__bytes_read.sum + dram__bytes_write.sum) of C3 slab launches
-# (1024 x 1024 x slab voxels x 1440 views of 2048^2, FP16): slab 128: 173.2 GB / 1.93e11
-# updates; slab 512: 938.8 GB / 7.73e11 updates
-BP_DRAM_BYTES_PER_UPDATE = {("c3", 128): (172.619e9 + 0.546e9) / (1024 * 1024 * 128 * 1440),
-                            ("c3", 512): (936.672e9 + 2.172e9) / (1024 * 1024 * 512 * 1440)}
+# ncu captures (dram__bytes_read.sum + dram__bytes_write.sum, one pass) of the C3 bench's
+# two 512-slice launches (1024 x 1024 x 512 voxels x 1440 views of 2048^2, FP16 storage):
+# 620.2 + 2.29 GB and 658.5 + 2.29 GB over 7.73e11 updates each
+BP_DRAM_BYTES_PER_UPDATE = {("c3", 512): ((620.229e9 + 2.292e9) + (658.527e9 + 2.288e9)) / 2
+                            / (1024 * 1024 * 512 * 1440)}
 
 
 # --------------------------------------------------------------------- clocks

@@ -168,19 +168,13 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                 float* ca_row = sacc[left ? jku : 0];
                 float* cb_row = sacc[right ? jku + 1 : 0];
                 if (z0 > z1) continue;
-                // steps (zb, qq): z = zb + qq + lane * sst for zb = z0, z0 + 32 sst, ...
-                // and qq < sst; each step's slice value is loaded one step ahead
-                int zb = z0, qq = 0;
-                float vz_next = z0 + lane * sst <= z1 ? __ldg(&col[z0 + lane * sst]) : 0.0f;
-                while (zb <= z1) {
-                    const int z = zb + qq + lane * sst;
-                    const float vz = vz_next;
-                    if (++qq == sst) {
-                        qq = 0;
-                        zb += kFR * sst;
-                    }
-                    const int zn = zb + qq + lane * sst;
-                    if (zb <= z1) vz_next = zn <= z1 ? __ldg(&col[zn]) : 0.0f;
+                // steps s = 0, 1, ...: zb = z0 + (s / sst) 32 sst, qq = s % sst,
+                // z = zb + qq + lane * sst. The slice values of the first kPre steps
+                // are loaded before any is used (kPre loads in flight per lane: the
+                // volume is far larger than L2), later ones one step ahead.
+                const int nsteps = ((z1 - z0) / (kFR * sst) + 1) * sst;
+                auto step_z = [&](int st) { return z0 + (st / sst) * kFR * sst + st % sst + lane * sst; };
+                auto add = [&](int z, float vz) {
                     int lr = -2;
                     float a0 = 0.0f, a1 = 0.0f, b0 = 0.0f, b1 = 0.0f;
                     if (z <= z1) {
@@ -202,6 +196,27 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                     if (left && in1) ca_row[p1] += a1;
                     if (right && in1) cb_row[p1] += b1;
                     __syncwarp();
+                };
+                constexpr int kPre = 8;
+                float pre[kPre];
+#pragma unroll
+                for (int st = 0; st < kPre; ++st) {
+                    const int z = step_z(st);
+                    pre[st] = (st < nsteps && z <= z1) ? __ldg(&col[z]) : 0.0f;
+                }
+#pragma unroll
+                for (int st = 0; st < kPre; ++st)
+                    if (st < nsteps) add(step_z(st), pre[st]);
+                if (nsteps > kPre) {
+                    int z = step_z(kPre);
+                    float vz_next = z <= z1 ? __ldg(&col[z]) : 0.0f;
+                    for (int st = kPre; st < nsteps; ++st) {
+                        const float vz = vz_next;
+                        const int zn = step_z(st + 1);
+                        if (st + 1 < nsteps) vz_next = zn <= z1 ? __ldg(&col[zn]) : 0.0f;
+                        add(z, vz);
+                        z = zn;
+                    }
                 }
             }
         }

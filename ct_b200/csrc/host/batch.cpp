@@ -32,11 +32,17 @@ struct ctb_batch {
     double ms32 = -1, ms16 = -1, ms8 = -1;   // best time per z voxels per thread
     std::vector<int> cand_zc, cand_nbuf;     // every timed candidate
     std::vector<double> cand_ms;
+    // side stream and events of the scans left out of the persistent kernel
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
     ~ctb_batch() {
         cudaSetDevice(device);
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         for (void* p : filtered) cudaFree(p);
         for (float4* p : views) cudaFree(p);
         cudaFree(d_desc);
@@ -84,16 +90,28 @@ int upload_plan(ctb_batch* b, cudaStream_t s) {
 int enqueue_batch(ctb_batch* b, cudaStream_t s) {
     int st = enqueue_filters(b, s);
     if (st != CTB_OK) return st;
+    // scans left out of the persistent kernel (box beyond its budget): one launch
+    // each, shared-memory kernel with its own buffer size when possible, else
+    // global gathers. They go on a side stream forked here, so their few long
+    // CTAs run beside the persistent kernel's instead of after it (the
+    // persistent kernel takes its work from a queue, so CTAs that start late
+    // only take fewer items); the side stream joins back before the end.
+    const bool fork = !b->plan.excluded.empty() && b->side;
+    cudaStream_t sx = fork ? b->side : s;
+    if (fork) {
+        CTB_CUDA_TRY(cudaEventRecord(b->ev_fork, s));
+        CTB_CUDA_TRY(cudaStreamWaitEvent(sx, b->ev_fork, 0));
+    }
+    for (int i : b->plan.excluded) {
+        st = backproject_launch(b->filtered[i], b->store, b->views[i], b->bp[i].n_views, b->bp[i].g, b->bp[i].hmax,
+                                b->bp[i].vol, 0, sx);
+        if (st != CTB_OK) return st;
+    }
+    if (fork) CTB_CUDA_TRY(cudaEventRecord(b->ev_join, sx));
     CTB_CUDA_TRY(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned long long), s));
     st = bp_batch_launch(b->plan, b->d_desc, b->d_tile_start, int(b->plan.included.size()), b->d_queue, s);
     if (st != CTB_OK) return st;
-    // scans left out of the persistent kernel (box beyond its budget): one launch each,
-    // shared-memory kernel with its own buffer size when possible, else global gathers
-    for (int i : b->plan.excluded) {
-        st = backproject_launch(b->filtered[i], b->store, b->views[i], b->bp[i].n_views, b->bp[i].g, b->bp[i].hmax,
-                                b->bp[i].vol, 0, s);
-        if (st != CTB_OK) return st;
-    }
+    if (fork) CTB_CUDA_TRY(cudaStreamWaitEvent(s, b->ev_join, 0));
     return CTB_OK;
 }
 
@@ -179,6 +197,12 @@ int ctb_batch_create(ctb_batch** out, int n, const ctb_scan* scans, int store_ty
         bs.vol = sc.vol;
         bs.accumulate = 0;
         b->bp.push_back(bs);
+    }
+    if (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(fail("ctb_batch_create: stream or events could not be created", CTB_ERR_CUDA));
     }
     if (cudaMalloc(&b->d_queue, sizeof(unsigned long long)) != cudaSuccess) {
         cudaGetLastError();

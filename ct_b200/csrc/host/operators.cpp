@@ -17,6 +17,17 @@
 
 namespace ctb {
 
+// A failed CUDA call ends the operation with CTB_ERR_CUDA and its message on
+// the context (ctb_last_error), as the facade's other operations do.
+#define OP_TRY(expr)                                                                              \
+    do {                                                                                          \
+        const cudaError_t _e = (expr);                                                            \
+        if (_e != cudaSuccess) {                                                                  \
+            cudaGetLastError();                                                                   \
+            return fail(CTB_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(_e));     \
+        }                                                                                         \
+    } while (0)
+
 namespace {
 constexpr size_t kSlabBytes = size_t(512) << 20;   // device slab buffer (volume slices)
 
@@ -64,7 +75,7 @@ int Reconstructor::op_prepare(int* slab) {
     const int dev = devices_.empty() ? 0 : devices_[0];
     if (!op_ || op_->device != dev) op_.reset(new OpWork(dev));
     OpWork& w = *op_;
-    CTB_CUDA_TRY(cudaSetDevice(dev));
+    OP_TRY(cudaSetDevice(dev));
     if (!w.s && cudaStreamCreateWithFlags(&w.s, cudaStreamNonBlocking) != cudaSuccess)
         return fail(CTB_ERR_CUDA, "stream creation failed");
     const int V = int(angles_.size());
@@ -80,8 +91,8 @@ int Reconstructor::op_prepare(int* slab) {
         (st = w.d_heights.ensure(sizeof(double) * V, "height offsets")) ||
         (st = w.d_sum.ensure(sizeof(double), "sum")))
         return fail(st, global_error());
-    CTB_CUDA_TRY(cudaMemcpyAsync(w.d_angles.p, angles_.data(), sizeof(double) * V, cudaMemcpyHostToDevice, w.s));
-    CTB_CUDA_TRY(cudaMemcpyAsync(w.d_heights.p, heights_px_.data(), sizeof(double) * V, cudaMemcpyHostToDevice, w.s));
+    OP_TRY(cudaMemcpyAsync(w.d_angles.p, angles_.data(), sizeof(double) * V, cudaMemcpyHostToDevice, w.s));
+    OP_TRY(cudaMemcpyAsync(w.d_heights.p, heights_px_.data(), sizeof(double) * V, cudaMemcpyHostToDevice, w.s));
     st = view_table_build(static_cast<const double*>(w.d_angles.p), static_cast<const double*>(w.d_heights.p), V,
                           static_cast<float4*>(w.d_views.p), w.s);
     return st == CTB_OK ? CTB_OK : fail(st, global_error());
@@ -95,11 +106,11 @@ int Reconstructor::op_forward(const float* host_vol, int slab) {
     const size_t plane = size_t(X) * Y;
     float* proj = static_cast<float*>(w.d_proj.p);
     float* dslab = static_cast<float*>(w.d_slab.p);
-    CTB_CUDA_TRY(cudaMemsetAsync(proj, 0, sizeof(float) * size_t(V) * det_.height * det_.width, w.s));
+    OP_TRY(cudaMemsetAsync(proj, 0, sizeof(float) * size_t(V) * det_.height * det_.width, w.s));
     for (int z0 = 0; z0 < Z; z0 += slab) {
         if (stop_) return fail(CTB_INTERRUPTED, "User interrupted. Stopping.");
         const int z1 = std::min(Z, z0 + slab);
-        CTB_CUDA_TRY(cudaMemcpyAsync(dslab, host_vol + plane * z0, sizeof(float) * plane * (z1 - z0),
+        OP_TRY(cudaMemcpyAsync(dslab, host_vol + plane * z0, sizeof(float) * plane * (z1 - z0),
                                      cudaMemcpyHostToDevice, w.s));
         const ProjGeom g = proj_geom(det_, grid_, z0, z1, 1.0f);
         const int st = forward_launch(dslab, static_cast<const float4*>(w.d_views.p), V, g, proj, 1, w.s);
@@ -125,9 +136,9 @@ int Reconstructor::op_backward(const float* d_proj, float* host_vol, float scale
         const int st = backproject_launch(d_proj, CTB_FP32, static_cast<const float4*>(w.d_views.p), V, g, hmax,
                                           dslab, 0, w.s);
         if (st != CTB_OK) return fail(st, global_error());
-        CTB_CUDA_TRY(cudaMemcpyAsync(host_vol + plane * z0, dslab, sizeof(float) * plane * (z1 - z0),
+        OP_TRY(cudaMemcpyAsync(host_vol + plane * z0, dslab, sizeof(float) * plane * (z1 - z0),
                                      cudaMemcpyDeviceToHost, w.s));
-        CTB_CUDA_TRY(cudaStreamSynchronize(w.s));
+        OP_TRY(cudaStreamSynchronize(w.s));
     }
     return CTB_OK;
 }
@@ -141,8 +152,8 @@ int Reconstructor::forward(const float* host_vol, float* host_proj) {
     if ((st = op_prepare(&slab)) != CTB_OK) return st;
     if ((st = op_forward(host_vol, slab)) != CTB_OK) return st;
     const size_t n = size_t(angles_.size()) * det_.height * det_.width;
-    CTB_CUDA_TRY(cudaMemcpyAsync(host_proj, op_->d_proj.p, sizeof(float) * n, cudaMemcpyDeviceToHost, op_->s));
-    CTB_CUDA_TRY(cudaStreamSynchronize(op_->s));
+    OP_TRY(cudaMemcpyAsync(host_proj, op_->d_proj.p, sizeof(float) * n, cudaMemcpyDeviceToHost, op_->s));
+    OP_TRY(cudaStreamSynchronize(op_->s));
     return CTB_OK;
 }
 
@@ -154,7 +165,7 @@ int Reconstructor::backward(const float* host_proj, float* host_vol) {
     int slab = 0, st;
     if ((st = op_prepare(&slab)) != CTB_OK) return st;
     const size_t n = size_t(angles_.size()) * det_.height * det_.width;
-    CTB_CUDA_TRY(cudaMemcpyAsync(op_->d_proj.p, host_proj, sizeof(float) * n, cudaMemcpyHostToDevice, op_->s));
+    OP_TRY(cudaMemcpyAsync(op_->d_proj.p, host_proj, sizeof(float) * n, cudaMemcpyHostToDevice, op_->s));
     if ((st = op_backward(static_cast<const float*>(op_->d_proj.p), host_vol, 1.0f, slab)) != CTB_OK) return st;
     if ((st = wait_status("the volume")) != CTB_OK) return fail(st, global_error());
     return CTB_OK;
@@ -171,14 +182,14 @@ int Reconstructor::gradient(const float* host_vol, const float* host_data, float
     const size_t n = size_t(angles_.size()) * det_.height * det_.width;
     if ((st = w.d_data.ensure(sizeof(float) * n, "measured projections")) != CTB_OK) return fail(st, global_error());
     if ((st = op_forward(host_vol, slab)) != CTB_OK) return st;
-    CTB_CUDA_TRY(cudaMemcpyAsync(w.d_data.p, host_data, sizeof(float) * n, cudaMemcpyHostToDevice, w.s));
-    CTB_CUDA_TRY(cudaMemsetAsync(w.d_sum.p, 0, sizeof(double), w.s));
+    OP_TRY(cudaMemcpyAsync(w.d_data.p, host_data, sizeof(float) * n, cudaMemcpyHostToDevice, w.s));
+    OP_TRY(cudaMemsetAsync(w.d_sum.p, 0, sizeof(double), w.s));
     float* r = static_cast<float*>(w.d_proj.p);
     if ((st = residual_launch(r, static_cast<const float*>(w.d_data.p), r, (long long)n,
                               static_cast<double*>(w.d_sum.p), w.s)) != CTB_OK)
         return fail(st, global_error());
     double sumsq = 0;
-    CTB_CUDA_TRY(cudaMemcpyAsync(&sumsq, w.d_sum.p, sizeof(double), cudaMemcpyDeviceToHost, w.s));
+    OP_TRY(cudaMemcpyAsync(&sumsq, w.d_sum.p, sizeof(double), cudaMemcpyDeviceToHost, w.s));
     // the backprojector's load scale of 2 gives 2 A^T r exactly (a power of two)
     if ((st = op_backward(r, host_grad, 2.0f, slab)) != CTB_OK) return st;
     if (f) *f = sumsq;

@@ -554,7 +554,7 @@ def facade_split(v, host_out, n, V, W, H, Z, Y, X, units, edge, vs, det, geom, r
     from ct_b200 import ops
     from ct_b200 import _lib as L
     one = host_out.clone()
-    v.setActiveCudaDevices([0] * n)
+    v.setActiveCudaDevices([0] * n)   # one-process leg, run at world size 1 only
     weights = np.full(n, 1.0 / n)
     begin = np.zeros(n + 1, np.int32)
     L.lib().ctb_split_slices(weights.ctypes.data, n, Z, begin.ctypes.data)
@@ -705,6 +705,7 @@ def run_ours(args):
         host_in.copy_(raw)
         host_out = torch.empty((Z, Y, X), dtype=torch.float32, pin_memory=True)
         v = CtVolume()
+        v.setActiveCudaDevices([local])   # this rank's GPU (the facade's default is device 0)
         v.setProjectionsPointer(host_in.data_ptr(), L.U16, V, W, H, angles, None, pixel_size=geom.pixel_eff,
                                 rotation="ccw", fcd_mm=geom.sod_mm, keep=host_in)
         v.setGrid(edge, edge, edge, vs)

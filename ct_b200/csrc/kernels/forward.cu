@@ -36,6 +36,7 @@
 // rows -> consecutive z) read contiguous memory.
 
 #include <algorithm>
+#include <type_traits>
 
 #include "../ctb_internal.h"
 #include "geom.cuh"
@@ -46,16 +47,15 @@ namespace {
 
 // a CTA: kFC warps, each kK detector columns x kFR * kRPL rows (kRPL per lane)
 constexpr int kFR = 32, kFC = 4, kK = 8, kRPL = 8;
-constexpr int kRows = kFR * kRPL, kStride = kRows + kRows / 32 + 1;
-__device__ __forceinline__ int rpos(int r) { return r + (r >> 5); }
+constexpr int kRows = kFR * kRPL, kStride = kRows + 1;
 constexpr unsigned kAll = 0xffffffffu;
 
 __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__ volz,
                                                        const float4* __restrict__ views, ProjGeom g,
                                                        float* __restrict__ proj, int accumulate) {
-    // per warp: columns c0 .. c0+7, rows R .. R + 255; row r sits at
-    // r + r / 32, so lanes whose rows are 2 apart (slices one pixel apart) hit
-    // 32 different banks
+    // per warp: columns c0 .. c0+7 of rows R .. R + 255, a column's rows
+    // contiguous, columns kStride = 257 floats apart (the eight columns of a
+    // row in eight banks for the write-out)
     __shared__ float s_rows[kFC][kK][kStride];
     const int lane = threadIdx.x;
     const int R = blockIdx.x * kRows;  // first row of the warp
@@ -165,59 +165,74 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                 const int sst = min(int(fminf(jinv, 1.0e7f) * 1.02f) + 1, max(1, g.Zs));
                 const float* col = volz + (long long)jcol * g.Zs;
                 const bool left = jku >= 0, right = jku + 1 < kK;
-                float* ca_row = sacc[left ? jku : 0];
-                float* cb_row = sacc[right ? jku + 1 : 0];
+                // accumulators of column u0 + 1 (used only when right); column u0's
+                // are kStride floats below (used only when left)
+                float* const cb = &sacc[0][0] + (jku + 1) * kStride;
                 if (z0 > z1) continue;
-                // steps s = 0, 1, ...: zb = z0 + (s / sst) 32 sst, qq = s % sst,
-                // z = zb + qq + lane * sst. The slice values of the first kPre steps
-                // are loaded before any is used (kPre loads in flight per lane: the
-                // volume is far larger than L2), later ones one step ahead.
-                const int nsteps = ((z1 - z0) / (kFR * sst) + 1) * sst;
-                auto step_z = [&](int st) { return z0 + (st / sst) * kFR * sst + st % sst + lane * sst; };
-                auto add = [&](int z, float vz) {
-                    int lr = -2;
-                    float a0 = 0.0f, a1 = 0.0f, b0 = 0.0f, b1 = 0.0f;
-                    if (z <= z1) {
-                        const float vi = row_at(rl, float(g.z_begin + z));
-                        const int v0 = int(vi);
-                        const float fv = __fsub_rn(vi, float(v0));
-                        const float va = jwa * vz, vb = jwb * vz;
-                        lr = v0 - R;
-                        a0 = (1.0f - fv) * va;  // row v0, column u0
-                        a1 = fv * va;           // row v0 + 1, column u0
-                        b0 = (1.0f - fv) * vb;  // row v0, column u0 + 1
-                        b1 = fv * vb;           // row v0 + 1, column u0 + 1
-                    }
-                    const bool in0 = lr >= 0 && lr < kRows, in1 = lr + 1 >= 0 && lr + 1 < kRows;
-                    const int p0 = rpos(lr), p1 = rpos(lr + 1);
-                    if (left && in0) ca_row[p0] += a0;
-                    if (right && in0) cb_row[p0] += b0;
+                const float2 jw2 = make_float2(jwa, jwb);
+                constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: floor of a float in [0, 2^22) by one add
+                auto add = [&](int z, float zf, float vz) {
+                    // computed for every lane; a lane past z1 writes nothing (lr = -2)
+                    const float vi = row_at(rl, zf);
+                    // int(vi) for vi > -1 (the rows of the slices walked here): the
+                    // magic-number add floors max(vi, 0)
+                    const float sm = __fadd_rz(fmaxf(vi, 0.0f), kMagic);
+                    const int v0 = __float_as_int(sm) - __float_as_int(kMagic);
+                    const float fv = __fsub_rn(vi, __fsub_rn(sm, kMagic));
+                    const float2 vab = __fmul2_rn(jw2, make_float2(vz, vz));
+                    const int lr = z <= z1 ? v0 - R : -2;
+                    const float f1 = 1.0f - fv;
+                    const float2 x0 = __fmul2_rn(make_float2(f1, f1), vab);  // row v0: columns u0, u0 + 1
+                    const float2 x1 = __fmul2_rn(make_float2(fv, fv), vab);  // row v0 + 1
+                    const bool in0 = unsigned(lr) < unsigned(kRows), in1 = unsigned(lr + 1) < unsigned(kRows);
+                    if (left && in0) cb[lr - kStride] += x0.x;
+                    if (right && in0) cb[lr] += x0.y;
                     __syncwarp();
-                    if (left && in1) ca_row[p1] += a1;
-                    if (right && in1) cb_row[p1] += b1;
+                    if (left && in1) cb[lr + 1 - kStride] += x1.x;
+                    if (right && in1) cb[lr + 1] += x1.y;
                     __syncwarp();
                 };
-                constexpr int kPre = 8;
-                float pre[kPre];
+                // slice of step st: z0 + lane s + (st / s) 32 s + st % s; the walk is
+                // compiled for s = 1 and s = 2 (the divisions become shifts and the
+                // preloaded steps' offsets constants) and for s at run time
+                auto walk = [&](auto s_c) {
+                    constexpr int S = decltype(s_c)::value;
+                    const int s = S > 0 ? S : sst;
+                    const int nsteps = ((z1 - z0) / (kFR * s) + 1) * s;
+                    const int zl = z0 + lane * s;
+                    const float zfl = float(g.z_begin + zl);
+                    auto off = [&](int st) { return (st / s) * kFR * s + st % s; };
+                    constexpr int kPre = 8;
+                    float pre[kPre];
 #pragma unroll
-                for (int st = 0; st < kPre; ++st) {
-                    const int z = step_z(st);
-                    pre[st] = (st < nsteps && z <= z1) ? __ldg(&col[z]) : 0.0f;
-                }
-#pragma unroll
-                for (int st = 0; st < kPre; ++st)
-                    if (st < nsteps) add(step_z(st), pre[st]);
-                if (nsteps > kPre) {
-                    int z = step_z(kPre);
-                    float vz_next = z <= z1 ? __ldg(&col[z]) : 0.0f;
-                    for (int st = kPre; st < nsteps; ++st) {
-                        const float vz = vz_next;
-                        const int zn = step_z(st + 1);
-                        if (st + 1 < nsteps) vz_next = zn <= z1 ? __ldg(&col[zn]) : 0.0f;
-                        add(z, vz);
-                        z = zn;
+                    for (int st = 0; st < kPre; ++st) {
+                        const int z = zl + off(st);
+                        pre[st] = (st < nsteps && z <= z1) ? __ldg(&col[z]) : 0.0f;
                     }
-                }
+#pragma unroll
+                    for (int st = 0; st < kPre; ++st)
+                        if (st < nsteps) {
+                            const int o = off(st);
+                            add(zl + o, zfl + float(o), pre[st]);
+                        }
+                    if (nsteps > kPre) {
+                        int o = off(kPre);
+                        float vz_next = zl + o <= z1 ? __ldg(&col[zl + o]) : 0.0f;
+                        for (int st = kPre; st < nsteps; ++st) {
+                            const float vz = vz_next;
+                            const int on = off(st + 1);
+                            if (st + 1 < nsteps) vz_next = zl + on <= z1 ? __ldg(&col[zl + on]) : 0.0f;
+                            add(zl + o, zfl + float(o), vz);
+                            o = on;
+                        }
+                    }
+                };
+                if (sst == 1)
+                    walk(std::integral_constant<int, 1>{});
+                else if (sst == 2)
+                    walk(std::integral_constant<int, 2>{});
+                else
+                    walk(std::integral_constant<int, 0>{});
             }
         }
     }
@@ -229,7 +244,7 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
         const int rk = R + r, ck = cs0 + k;
         if (rk >= g.H || ck >= g.W) continue;
         float* out = proj + (long long)iv * g.view_stride + (long long)rk * g.W + ck;
-        const float acc = sacc[k][rpos(r)];
+        const float acc = sacc[k][r];
         *out = accumulate ? (*out + acc) : acc;
     }
 }
@@ -251,6 +266,7 @@ int forward_launch(const float* vol, const float4* views, int n_views, const Pro
     if (st == CTB_OK) {
         dim3 block(kFR, kFC, 1);
         dim3 grid((g.H + kRows - 1) / kRows, (g.W + kFC * kK - 1) / (kFC * kK), n_views);
+        cudaFuncSetAttribute(fp_kernel, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         fp_kernel<<<grid, block, 0, s>>>(volz, views, g, proj, accumulate);
         st = cuda_status(cudaGetLastError(), "fp_kernel launch");
     }

@@ -202,7 +202,10 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                     const int zl = z0 + lane * s;
                     const float zfl = float(g.z_begin + zl);
                     auto off = [&](int st) { return (st / s) * kFR * s + st % s; };
-                    constexpr int kPre = 8;
+                    // the slice values of the first kPre steps are loaded before any
+                    // is used (a 256-row band is about 8 steps at s = 1 and 10 at
+                    // s = 2), later ones one step ahead
+                    constexpr int kPre = 10;
                     float pre[kPre];
 #pragma unroll
                     for (int st = 0; st < kPre; ++st) {

@@ -278,6 +278,11 @@ def adjoint_case(V=36, H=20, W=30, grid_size=None, vs=1.0, rel=None, uoff=0.0, h
     dict(grid_size=(14, 16, 18), vs=2.0),
     dict(grid_size=(25, 21, 9), vs=1.3, heights=True),
     dict(V=50, H=33, W=47, seed=2),
+    # tall slabs of fine slices: the forward projector's walk with the slice
+    # spacing at run time (rows 0.3 apart, spacing 4) and at spacing 2 (rows
+    # 0.7 apart), both with more steps per column than it preloads
+    dict(V=12, H=120, W=24, grid_size=(8, 8, 320), vs=0.3, seed=3),
+    dict(V=12, H=250, W=16, grid_size=(6, 6, 340), vs=0.7, heights=True, seed=4),
 ])
 def test_dot_product_adjoint(case):
     det, grid, ang, h, x, y = adjoint_case(**case)

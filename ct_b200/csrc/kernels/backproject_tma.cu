@@ -119,9 +119,14 @@ template <> __device__ __forceinline__ float sub_from<__nv_bfloat16>(__nv_bfloat
     return d;
 }
 
-template <typename T, int ZC>
-__device__ __forceinline__ void column_pairs(const T* col, const int BU, const float* zf, float mdv, float c0,
+// KBU > 0: the box row stride as a compile-time constant (the loads of row
+// v0 + 1 then take it as an immediate offset instead of an added register:
+// 2-3 % faster for FP16, 4 % for FP32 on 1440 views of 2048^2 into 1024^3,
+// bit-identical).
+template <typename T, int ZC, int KBU = 0>
+__device__ __forceinline__ void column_pairs(const T* col, const int BU_run, const float* zf, float mdv, float c0,
                                              float fu, float w, float* acc, BoxRows br) {
+    const int BU = KBU > 0 ? KBU : BU_run;
     constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
     const float2 mdv2 = make_float2(mdv, mdv), c02 = make_float2(c0, c0);
     const float2 fu2 = make_float2(fu, fu), w2 = make_float2(w, w);
@@ -156,6 +161,25 @@ __device__ __forceinline__ void column_pairs(const T* col, const int BU, const f
         acc[j] = s.x;
         acc[j + 1] = s.y;
     }
+}
+
+// column_pairs with the two most common row strides compiled in (box_dims
+// gives 128 bytes times k plus 32: 80 or 144 texels of 16 bits, 72 or 40 of
+// 32 bits for voxels of one to two detector pixels), any other at run time.
+// An if-chain: a switch over more strides (a jump table) was 1 % slower.
+template <typename T, int ZC>
+__device__ __forceinline__ void column_pairs_any(const T* col, const int BU, const float* zf, float mdv, float c0,
+                                                 float fu, float w, float* acc, BoxRows br) {
+    constexpr int kA = sizeof(T) == 4 ? 72 : 80, kB = sizeof(T) == 4 ? 40 : 144;
+    if (BU == kA) {
+        column_pairs<T, ZC, kA>(col, BU, zf, mdv, c0, fu, w, acc, br);
+        return;
+    }
+    if (BU == kB) {
+        column_pairs<T, ZC, kB>(col, BU, zf, mdv, c0, fu, w, acc, br);
+        return;
+    }
+    column_pairs<T, ZC>(col, BU, zf, mdv, c0, fu, w, acc, br);
 }
 
 template <typename T> __device__ __forceinline__ float gval(const T* p);
@@ -357,7 +381,7 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                     // the per-voxel membership test, so this loop and the checked one take the same
                     // decisions
                     if (fminf(vf, vl) >= 0.5f && fmaxf(vf, vl) <= g.vi_hi - 0.5f) {
-                        column_pairs<T, ZC>(col, BU, zf, rl.mdv, rl.c0, fu, w, acc, BoxRows{o.y, bx.BV});
+                        column_pairs_any<T, ZC>(col, BU, zf, rl.mdv, rl.c0, fu, w, acc, BoxRows{o.y, bx.BV});
                     } else {
                         int ja, jb;
                         v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);

@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(kBX * kBY) bp_kernel(const T* __restrict__ pro
             const RowLine rl = row_line(U, q.z, g.zpv, g.vs, g.vPre);
 #pragma unroll
             for (int j = 0; j < ZC; ++j) {
-                const float vi = row_at(rl, float(g.z_begin + z0 + j));
+                const float vi = row_at(rl, g.z_begin + z0 + j);
                 const float zw = __fmul_rn(__fsub_rn(float(z0 + j), g.zPre), g.vs);
                 if (v_inside(zw, q.z, U, g.lbV, g.ubV)) {
                     int v0 = int(vi);

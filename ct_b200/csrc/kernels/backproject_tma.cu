@@ -123,17 +123,28 @@ template <> __device__ __forceinline__ float sub_from<__nv_bfloat16>(__nv_bfloat
 // v0 + 1 then take it as an immediate offset instead of an added register:
 // 2-3 % faster for FP16, 4 % for FP32 on 1440 views of 2048^2 into 1024^3,
 // bit-identical).
-template <typename T, int ZC, int KBU = 0>
-__device__ __forceinline__ void column_pairs(const T* col, const int BU_run, const float* zf, float mdv, float c0,
+// The tile's first slice sits OFF slices into its block of 32 (geom.cuh), whose
+// row origin is c0b: slice j's row is fma(OFF + j, mdv, c0b). IMM: OFF + j is
+// an immediate operand and no register holds the slices' offsets (the freed
+// registers let the compiler overlap voxel pairs: 4-6 % faster); otherwise
+// the offsets zo[j] = OFF + j come from registers (the persistent batch
+// kernel, whose extra state would otherwise spill), with the same values.
+template <typename T, int ZC, int KBU, int OFF, bool IMM>
+__device__ __forceinline__ void column_pairs(const T* col, const int BU_run, const float* zo, float c0b, float mdv,
                                              float fu, float w, float* acc, BoxRows br) {
+    static_assert(OFF % ZC == 0 && OFF + ZC <= 32, "a tile lies inside one block of 32 slices");
     const int BU = KBU > 0 ? KBU : BU_run;
     constexpr float kMagic = 12582912.0f;   // 1.5 * 2^23
-    const float2 mdv2 = make_float2(mdv, mdv), c02 = make_float2(c0, c0);
     const float2 fu2 = make_float2(fu, fu), w2 = make_float2(w, w);
     const float2 m1 = make_float2(-1.0f, -1.0f), mg = make_float2(kMagic, kMagic);
+    const float2 mdv2 = make_float2(mdv, mdv), c0b2 = make_float2(c0b, c0b);
 #pragma unroll
     for (int j = 0; j < ZC; j += 2) {
-        const float2 vi = __ffma2_rn(make_float2(zf[j], zf[j + 1]), mdv2, c02);
+        float2 vi;
+        if constexpr (IMM)
+            vi = make_float2(fmaf(float(OFF + j), mdv, c0b), fmaf(float(OFF + j + 1), mdv, c0b));
+        else
+            vi = __ffma2_rn(make_float2(zo[j], zo[j + 1]), mdv2, c0b2);
         const float2 sm = __fadd2_rz(vi, mg);
         const float2 nfl = __ffma2_rn(sm, m1, mg);   // -float(floor(vi))
         const float2 fv = __fadd2_rn(vi, nfl);
@@ -167,19 +178,36 @@ __device__ __forceinline__ void column_pairs(const T* col, const int BU_run, con
 // gives 128 bytes times k plus 32: 80 or 144 texels of 16 bits, 72 or 40 of
 // 32 bits for voxels of one to two detector pixels), any other at run time.
 // An if-chain: a switch over more strides (a jump table) was 1 % slower.
-template <typename T, int ZC>
-__device__ __forceinline__ void column_pairs_any(const T* col, const int BU, const float* zf, float mdv, float c0,
-                                                 float fu, float w, float* acc, BoxRows br) {
+template <typename T, int ZC, int OFF, bool IMM>
+__device__ __forceinline__ void column_pairs_bu(const T* col, const int BU, const float* zo, float c0b, float mdv,
+                                                float fu, float w, float* acc, BoxRows br) {
     constexpr int kA = sizeof(T) == 4 ? 72 : 80, kB = sizeof(T) == 4 ? 40 : 144;
     if (BU == kA) {
-        column_pairs<T, ZC, kA>(col, BU, zf, mdv, c0, fu, w, acc, br);
+        column_pairs<T, ZC, kA, OFF, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
         return;
     }
     if (BU == kB) {
-        column_pairs<T, ZC, kB>(col, BU, zf, mdv, c0, fu, w, acc, br);
+        column_pairs<T, ZC, kB, OFF, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
         return;
     }
-    column_pairs<T, ZC>(col, BU, zf, mdv, c0, fu, w, acc, br);
+    column_pairs<T, ZC, 0, OFF, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
+}
+
+// the pair loop for a tile at offset off (a multiple of ZC below 32) in its block
+template <typename T, int ZC, bool IMM>
+__device__ __forceinline__ void column_pairs_any(const T* col, const int BU, int off, const float* zo, float c0b,
+                                                 float mdv, float fu, float w, float* acc, BoxRows br) {
+    if constexpr (ZC >= 32 || !IMM) {
+        column_pairs_bu<T, ZC, 0, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
+    } else if constexpr (ZC == 16) {
+        if (off == 0) column_pairs_bu<T, ZC, 0, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
+        else column_pairs_bu<T, ZC, 16, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
+    } else {
+        if (off == 0) column_pairs_bu<T, ZC, 0, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
+        else if (off == 8) column_pairs_bu<T, ZC, 8, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
+        else if (off == 16) column_pairs_bu<T, ZC, 16, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
+        else column_pairs_bu<T, ZC, 24, IMM>(col, BU, zo, c0b, mdv, fu, w, acc, br);
+    }
 }
 
 template <typename T> __device__ __forceinline__ float gval(const T* p);
@@ -237,12 +265,12 @@ __device__ __forceinline__ bool aborted(const volatile int* f) { return *f != 0;
 // tiles that start later start further on, so the CTAs resident at one time
 // read the same few views and share them in L2 (2.3x less DRAM traffic on a
 // 1024^3 slab of 1440 views of 2048^2).
-template <typename T, int ZC, int NBUF>
+template <typename T, int ZC, int NBUF, bool IMM>
 __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __restrict__ proj,
                                           const float4* __restrict__ views, int n_views, const ProjGeom& g,
                                           const Box& bx, int buf_stride, float* __restrict__ vol, int accumulate,
                                           int tile_x, int tile_y, int tile_z, Pipe<NBUF>& p, T* buf,
-                                          unsigned& seq, int rot) {
+                                          unsigned& seq, int rot, int zshift) {
     volatile int* abort_flag = &p.abort_flag;
     // Consumer warp w covers an 8 (x) x 4 (y) patch of columns: its lanes then
     // sample a compact patch of the box (a few rows x ~12 words), which keeps
@@ -251,11 +279,15 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const bool producer = warp == kConsumerWarps;
-    const int x0 = tile_x * kTX, y0 = tile_y * kTY, z0 = tile_z * ZC;
+    // z tiles start on multiples of ZC box slices (so each lies inside one block of
+    // 32 slices, geom.cuh): zshift = z_begin mod ZC, and the first tile of a slab
+    // that starts off such a multiple begins before the slab, its slices there
+    // computed but not stored (the batch kernel's slabs start at 0: zshift 0)
+    const int x0 = tile_x * kTX, y0 = tile_y * kTY, z0 = tile_z * ZC - zshift;
     constexpr int kWX = kTX / 8;   // warps along x
     const int x = x0 + (warp % kWX) * 8 + (lane & 7), y = y0 + (warp / kWX) * 4 + (lane >> 3);
     const int x1 = min(x0 + kTX, g.X) - 1, y1 = min(y0 + kTY, g.Y) - 1;
-    const int zl = min(ZC, g.Zs - z0);  // voxels of this tile in the slab
+    const int zf = zshift > 0 ? max(0, -z0) : 0, zl = min(ZC, g.Zs - z0);  // voxels zf .. zl-1 are in the slab
     const long long plane = (long long)g.X * g.Y;
 
     // A tile whose closest column lies outside the reconstruction cylinder has
@@ -266,8 +298,8 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
         const float dx = fmaxf(0.0f, fmaxf(ax, -bxw)), dy = fmaxf(0.0f, fmaxf(ay, -byw));
         if (dx * dx + dy * dy > g.r2 * 1.0001f + 1.0f) {
             if (!producer && !accumulate && x < g.X && y < g.Y) {
-                float* out = vol + (long long)z0 * plane + (long long)y * g.X + x;
-                for (int j = 0; j < zl; ++j) out[j * plane] = 0.0f;
+                float* out = vol + (long long)y * g.X + x;
+                for (int j = zf; j < zl; ++j) out[(long long)(z0 + j) * plane] = 0.0f;
             }
             return;
         }
@@ -276,9 +308,13 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
     const float yw = world_coord(y, g.yPre, g.vs);
     const bool live = !producer && x < g.X && y < g.Y && in_cylinder(xw, yw, g.r2);
 
-    float zf[ZC];
+    // the tile's first box slice and its offset in its block of 32 slices
+    // (a multiple of ZC: the tile lies inside the block)
+    const int zt = g.z_begin + z0, zoff = zt & 31;
+    const float fzoff = float(zoff);
+    float zo[ZC];   // slice offsets in the block for the register form of the pair loop
 #pragma unroll
-    for (int j = 0; j < ZC; ++j) zf[j] = float(g.z_begin + z0 + j);
+    for (int j = 0; j < ZC; ++j) zo[j] = fzoff + float(j);
 
     if (producer) {
         // ------------------------------------------------------------ producer
@@ -309,7 +345,7 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                 column_geom(world_coord(cx, g.xPre, g.vs), world_coord(cy, g.yPre, g.vs), q.x, q.y, g.D, g.uOff,
                             &U, &u);
                 const RowLine rl = row_line(U, q.z, g.zpv, g.vs, g.vPre);
-                const float va = row_at(rl, zf[0]), vb = row_at(rl, zf[ZC - 1]);
+                const float va = row_at(rl, zt), vb = row_at(rl, zt + ZC - 1);
                 umin = umax = __fadd_rn(u, g.uPre);
                 vmin = fminf(va, vb);
                 vmax = fmaxf(va, vb);
@@ -368,7 +404,10 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                 const int u0 = int(ui);
                 const float fu = __fsub_rn(ui, float(u0));
                 const RowLine rl = row_line(U, q.z, g.zpv, g.vs, g.vPre);
-                const float vf = row_at(rl, zf[0]), vl = row_at(rl, zf[ZC - 1]);
+                const float c0b = row_block(rl, zt - zoff);
+                // row_at(rl, zt + j): slice j sits zoff + j < 32 slices into the block
+                auto row_j = [&](int j) { return fmaf(fzoff + float(j), rl.mdv, c0b); };
+                const float vf = row_j(0), vl = row_j(ZC - 1);
                 if (!p.ovf[b]) {
                     const int2 o = p.org[b];
                     int cu = u0 - o.x;   // column of u0 in the box
@@ -381,13 +420,14 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                     // the per-voxel membership test, so this loop and the checked one take the same
                     // decisions
                     if (fminf(vf, vl) >= 0.5f && fmaxf(vf, vl) <= g.vi_hi - 0.5f) {
-                        column_pairs_any<T, ZC>(col, BU, zf, rl.mdv, rl.c0, fu, w, acc, BoxRows{o.y, bx.BV});
+                        column_pairs_any<T, ZC, IMM>(col, BU, zoff, zo, c0b, rl.mdv, fu, w, acc,
+                                                     BoxRows{o.y, bx.BV});
                     } else {
                         int ja, jb;
                         v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);
 #pragma unroll
                         for (int j = 0; j < ZC; ++j) {
-                            const float vi = row_at(rl, zf[j]);
+                            const float vi = row_j(j);
                             if (j >= ja && j <= jb) {
                                 int v0 = int(vi);
                                 const float fv = __fsub_rn(vi, float(v0));
@@ -414,7 +454,7 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
                     v_inside_run(z0, ZC, g.zPre, g.vs, q.z, U, g.lbV, g.ubV, &ja, &jb);
 #pragma unroll
                     for (int j = 0; j < ZC; ++j) {
-                        const float vi = row_at(rl, zf[j]);
+                        const float vi = row_j(j);
                         if (j >= ja && j <= jb) {
                             int v0 = int(vi);
                             const float fv = __fsub_rn(vi, float(v0));
@@ -436,10 +476,11 @@ __device__ __forceinline__ void tile_pass(const CUtensorMap* map, const T* __res
     }
     seq += n_views;
     if (aborted(abort_flag) || x >= g.X || y >= g.Y) return;
+    // (slice z0 + j of column (x, y); z0 < 0 only for slices j < zf, which are not stored)
     float* out = vol + (long long)z0 * plane + (long long)y * g.X + x;
 #pragma unroll
     for (int j = 0; j < ZC; ++j) {
-        if (j < zl) {
+        if (j >= zf && j < zl) {
             float* o = out + j * plane;
             *o = accumulate ? (*o + acc[j]) : acc[j];
         }
@@ -473,8 +514,8 @@ __global__ void __launch_bounds__(kThreads, ZC > 16 ? 3 : 4) bp_tma_kernel(const
     // k / resident of a tile's time after the first, so it starts that far on
     const long long k = blockIdx.x + (long long)gridDim.x * (blockIdx.y + (long long)gridDim.y * blockIdx.z);
     const int rot = int((k % resident) * n_views / resident);
-    tile_pass<T, ZC, NBUF>(&map, proj, views, n_views, g, bx, bx.buf_elems, vol, accumulate, blockIdx.x,
-                           blockIdx.y, blockIdx.z, p, reinterpret_cast<T*>(smem_raw), seq, rot);
+    tile_pass<T, ZC, NBUF, true>(&map, proj, views, n_views, g, bx, bx.buf_elems, vol, accumulate, blockIdx.x,
+                           blockIdx.y, blockIdx.z, p, reinterpret_cast<T*>(smem_raw), seq, rot, g.z_begin % ZC);
     __syncthreads();
     if (threadIdx.x == kConsumerWarps * 32 && p.abort_flag) pipe_abort_drain(p, seq);
 }
@@ -535,9 +576,9 @@ __global__ void __launch_bounds__(kThreads, ZC > 16 ? 3 : 4) bp_batch_kernel(con
         if (p.item >= total || p.abort_flag) break;
         const ScanDesc& d = scans[s_scan];
         const int rot = int((p.item % gridDim.x) * d.n_views / gridDim.x);
-        tile_pass<T, ZC, NBUF>(&d.map, static_cast<const T*>(d.proj), d.views, d.n_views, sg, sbx, buf_stride,
+        tile_pass<T, ZC, NBUF, false>(&d.map, static_cast<const T*>(d.proj), d.views, d.n_views, sg, sbx, buf_stride,
                                d.vol, d.accumulate, s_tile[0], s_tile[1], s_tile[2], p,
-                               reinterpret_cast<T*>(smem_raw), seq, rot);
+                               reinterpret_cast<T*>(smem_raw), seq, rot, 0);
         __syncthreads();
     }
     if (threadIdx.x == kConsumerWarps * 32 && p.abort_flag) pipe_abort_drain(p, seq);
@@ -591,7 +632,7 @@ bool box_dims(const ProjGeom& g, int ZC, double hmax, int esize, Box* b) {
     }
     uext += 0.05;
     const double zabs =
-        std::max(std::fabs((0 - g.zPre) * vs), std::fabs((g.Zs + ZC - 1 - g.zPre) * vs)) + hmax;
+        std::max(std::fabs((-(ZC - 1) - g.zPre) * vs), std::fabs((g.Zs + ZC - 1 - g.zPre) * vs)) + hmax;
     const double vext = (ZC - 1) * vs * Umax + zabs * dU * T;
     // Row stride: 32 bytes more than a multiple of 128, so adjacent box rows
     // sit 8 banks apart and only rows four apart in one column share a bank;
@@ -659,7 +700,7 @@ int launch_t(const T* proj, const float4* views, int n_views, const ProjGeom& g,
     if (smem > 200 * 1024) return CTB_ERR_UNSUPPORTED;
     auto kern = nbuf == 4 ? bp_tma_kernel<T, ZC, 4> : nbuf == 3 ? bp_tma_kernel<T, ZC, 3> : bp_tma_kernel<T, ZC, 2>;
     if (const int st = ensure_dynamic_smem(reinterpret_cast<const void*>(kern), smem)) return st;
-    dim3 grid((g.X + kTX - 1) / kTX, (g.Y + kTY - 1) / kTY, (g.Zs + ZC - 1) / ZC);
+    dim3 grid((g.X + kTX - 1) / kTX, (g.Y + kTY - 1) / kTY, (g.Zs + g.z_begin % ZC + ZC - 1) / ZC);
     if (grid.y > 65535 || grid.z > 65535) return CTB_ERR_UNSUPPORTED;
     int per_sm = 0, dev = 0, sms = 0;
     CTB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem));
@@ -697,7 +738,9 @@ int batch_plan_t(const BpBatchScan* scans, int n, BpBatchPlan* plan, int nbuf_re
         // a scan whose box would push it below its CTAs per SM (four, or three at
         // 32 z voxels per thread; three buffers each) runs through its own launch.
         constexpr size_t kBoxBudget = (227 * 1024 / (ZC > 16 ? 3 : 4) - 2048) / 3;
-        if (!box_dims(sc.g, ZC, sc.hmax, sizeof(T), &d.bx) || size_t(d.bx.buf_elems) * sizeof(T) > kBoxBudget ||
+        // (its tiles start at slice 0 of the slab: a slab off a multiple of 32 runs on its own too)
+        if (sc.g.z_begin % 32 != 0 || !box_dims(sc.g, ZC, sc.hmax, sizeof(T), &d.bx) ||
+            size_t(d.bx.buf_elems) * sizeof(T) > kBoxBudget ||
             !make_map((const T*)sc.proj, sc.n_views, sc.g, d.bx, &d.map)) {
             plan->excluded.push_back(i);
             continue;

@@ -1,6 +1,8 @@
 // Matched forward projector: the exact transpose of the voxel-driven
 // backprojector in backproject.cu (no counterpart in the reference, which has
-// no forward model).
+// no forward model). The shared-memory backprojector takes the same decisions
+// but for rows whose coordinate lies within one unit in the last place of an
+// integer (geom.cuh), so against it the transpose holds to that rounding.
 //
 // The backprojector adds, for every voxel and view,
 //     w * [(1-fv)((1-fu) p[v0][u0] + fu p[v0][u0+1]) + fv((1-fu) p[v0+1][u0] + fu p[v0+1][u0+1])]
@@ -19,7 +21,8 @@
 //     linear functions) and gets a short range of candidate columns;
 //  2. step by step through those ranges, each lane evaluates one candidate
 //     column with the very same FP32 expressions as the backprojector (so the
-//     discrete decisions u0, v0 and the masks agree bit for bit), and for a
+//     discrete decisions u0, v0 and the masks agree bit for bit with the
+//     gather kernel's), and for a
 //     column that reaches the strip (u0 in c0-1 .. c0+7) its run of slices
 //     inside the detector rows (the reference's v test, once per column);
 //  3. the columns that reach the strip are broadcast one at a time (ballot +
@@ -171,9 +174,11 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                 if (z0 > z1) continue;
                 const float2 jw2 = make_float2(jwa, jwb);
                 constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: floor of a float in [0, 2^22) by one add
-                auto add = [&](int z, float zf, float vz) {
-                    // computed for every lane; a lane past z1 writes nothing (lr = -2)
-                    const float vi = row_at(rl, zf);
+                auto add = [&](int z, float fo, float c0b, float vz) {
+                    // computed for every lane; a lane past z1 writes nothing (lr = -2).
+                    // The row as geom.cuh forms it: fo = z mod 32 (box slice z), c0b
+                    // the row origin of z's block of 32 slices
+                    const float vi = fmaf(fo, rl.mdv, c0b);
                     // int(vi) for vi > -1 (the rows of the slices walked here): the
                     // magic-number add floors max(vi, 0)
                     const float sm = __fadd_rz(fmaxf(vi, 0.0f), kMagic);
@@ -200,8 +205,28 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                     const int s = S > 0 ? S : sst;
                     const int nsteps = ((z1 - z0) / (kFR * s) + 1) * s;
                     const int zl = z0 + lane * s;
-                    const float zfl = float(g.z_begin + zl);
                     auto off = [&](int st) { return (st / s) * kFR * s + st % s; };
+                    // row arguments of step st: box slice za + off(st) = za + p + 32 s k
+                    // (p = st % s, k = st / s) sits where za + p sits in its block of
+                    // 32 slices, and that block starts 32 s k slices later
+                    const int za = g.z_begin + zl;
+                    const int zo0 = za & 31, zo1 = (za + 1) & 31;
+                    const float fo0 = float(zo0), fb0 = float(za - zo0);
+                    const float fo1 = float(zo1), fb1 = float(za + 1 - zo1);
+                    auto rowarg = [&](int st, float& fo, float& c0b) {
+                        if constexpr (S == 1) {
+                            fo = fo0;
+                            c0b = fmaf(fb0 + float(kFR * st), rl.mdv, rl.c0);
+                        } else if constexpr (S == 2) {
+                            const bool odd = st & 1;
+                            fo = odd ? fo1 : fo0;
+                            c0b = fmaf((odd ? fb1 : fb0) + float(2 * kFR * (st >> 1)), rl.mdv, rl.c0);
+                        } else {
+                            const int zz = za + off(st), zo = zz & 31;
+                            fo = float(zo);
+                            c0b = row_block(rl, zz - zo);
+                        }
+                    };
                     // the slice values of the first kPre steps are loaded before any
                     // is used (a 256-row band is about 8 steps at s = 1 and 10 at
                     // s = 2), later ones one step ahead
@@ -215,8 +240,9 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
 #pragma unroll
                     for (int st = 0; st < kPre; ++st)
                         if (st < nsteps) {
-                            const int o = off(st);
-                            add(zl + o, zfl + float(o), pre[st]);
+                            float fo, c0b;
+                            rowarg(st, fo, c0b);
+                            add(zl + off(st), fo, c0b, pre[st]);
                         }
                     if (nsteps > kPre) {
                         int o = off(kPre);
@@ -225,7 +251,9 @@ __global__ void __launch_bounds__(kFR * kFC) fp_kernel(const float* __restrict__
                             const float vz = vz_next;
                             const int on = off(st + 1);
                             if (st + 1 < nsteps) vz_next = zl + on <= z1 ? __ldg(&col[zl + on]) : 0.0f;
-                            add(zl + o, zfl + float(o), vz);
+                            float fo, c0b;
+                            rowarg(st, fo, c0b);
+                            add(zl + o, fo, c0b, vz);
                             o = on;
                         }
                     }

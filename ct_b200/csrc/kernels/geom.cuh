@@ -51,10 +51,17 @@ __device__ __forceinline__ void column_geom(float xw, float yw, float sn, float 
 }
 
 // Detector row coordinate of a voxel, vi = H/2 - (zw + h) U (:1008, :1014),
-// as a line in the box voxel index z: vi(z) = fma(z, mdv, c0) with
-// zw = (z - zPre) vs, mdv = -vs U and c0 = H/2 - (h - zPre vs) U. One fused
-// multiply-add per voxel; the backprojectors and the forward projector all use
-// exactly this form so that they take the same row decisions.
+// as a line in the box voxel index z: vi(z) = z mdv + c0 with zw = (z - zPre)
+// vs, mdv = -vs U and c0 = H/2 - (h - zPre vs) U, evaluated from the start of
+// z's block of 32 slices:
+//     vi(z) = fma(z mod 32, mdv, fma(z - z mod 32, mdv, c0)).
+// Every path (the backprojectors' pair loop and per-voxel loops, the gather
+// backprojector, the forward projector) forms rows this way, so they take the
+// same row decisions for any slab or tile split. The block origin lets the
+// shared-memory backprojector's pair loop, whose tiles of 32 slices start on
+// a block, take z mod 32 as an immediate operand with one row origin per
+// view, instead of holding 32 slice coordinates in registers (the freed
+// registers let the compiler overlap voxel pairs: 6 % faster for FP16).
 struct RowLine {
     float mdv, c0;
 };
@@ -66,12 +73,19 @@ __device__ __forceinline__ RowLine row_line(float U, float h, float zpv, float v
     return r;
 }
 
-__device__ __forceinline__ float row_at(const RowLine& r, float zf) { return fmaf(zf, r.mdv, r.c0); }
+// row origin of the block of 32 slices that starts at box slice zb (a multiple of 32)
+__device__ __forceinline__ float row_block(const RowLine& r, int zb) { return fmaf(float(zb), r.mdv, r.c0); }
+
+// row of box slice z (z >= 0)
+__device__ __forceinline__ float row_at(const RowLine& r, int z) {
+    const int zo = z & 31;
+    return fmaf(float(zo), r.mdv, row_block(r, z - zo));
+}
 
 // Whether a voxel falls inside the detector's rows, decided exactly as the
 // reference decides it (:926-928, :1008-1011): v = (z + h) U rounded in float
 // and kept when lbV <= v <= ubV, with zw the voxel's world z. The row line
-// above gives the row and its weight; near the first and last row its single
+// above gives the row and its weight; near the first and last row its
 // rounding can land on the other side of a bound that the reference's v hits
 // exactly (a voxel whose v equals ubV, row 0), so membership is taken from
 // here. A kept voxel's row line value then lies within rounding of [0, H-1.1],

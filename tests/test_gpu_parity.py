@@ -369,28 +369,57 @@ def test_progress_previews(tmp_path):
     assert not first[:Z - 32].any()
 
 
+TRANSPOSE_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, %r)
+from ct_b200 import ops
+vs, uoff, heights, out = float(sys.argv[1]), float(sys.argv[2]), sys.argv[3] == "1", sys.argv[4]
+V, H, W, n = 3, 14, 16, 6
+rng = np.random.default_rng(int(vs * 10))
+det, _ = ops.detector(W, H, 40.0, u_offset=uoff)
+grid = ops.custom_grid(det, (n, n, n), vs)
+ang = rng.uniform(0, 360, V)
+h = rng.uniform(-1.5, 1.5, V) if heights else None
+A = np.zeros((V * H * W, n * n * n))
+for k in range(n * n * n):
+    e = torch.zeros(n * n * n, device="cuda")
+    e[k] = 1.0
+    A[:, k] = ops.forward_project(e.view(n, n, n), ang, h, det, grid).cpu().numpy().ravel()
+At = np.zeros((n * n * n, V * H * W))
+for k in range(V * H * W):
+    e = torch.zeros(V * H * W, device="cuda")
+    e[k] = 1.0
+    At[:, k] = ops.backproject(e.view(V, H, W), ang, h, det, grid).cpu().numpy().ravel()
+np.save(out + "_A.npy", A)
+np.save(out + "_At.npy", At)
+"""
+
+
+def transpose_matrices(tmp_path, variant, vs, uoff, heights):
+    """A (forward projector, unit volumes) and A^T (backprojector forced to `variant`, unit pixels)."""
+    import subprocess
+    import sys
+    out = str(tmp_path / f"{variant}_{vs}")
+    env = dict(os.environ, CTB_BP_VARIANT=variant)
+    r = subprocess.run([sys.executable, "-c", TRANSPOSE_SCRIPT % ROOT, str(vs), str(uoff), "1" if heights else "0",
+                        out], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-3000:]
+    return np.load(out + "_A.npy"), np.load(out + "_At.npy")
+
+
 @pytest.mark.parametrize("vs,uoff,heights", [(1.0, 0.0, False), (0.6, 1.5, True), (2.5, -2.0, False)])
-def test_forward_is_the_exact_transpose(vs, uoff, heights):
-    """Every matrix element: A e_voxel (forward projector) against A^T e_pixel (backprojector)."""
-    V, H, W, n = 3, 14, 16, 6
-    rng = np.random.default_rng(int(vs * 10))
-    det, _ = ops.detector(W, H, 40.0, u_offset=uoff)
-    grid = ops.custom_grid(det, (n, n, n), vs)
-    ang = rng.uniform(0, 360, V)
-    h = rng.uniform(-1.5, 1.5, V) if heights else None
-    A = np.zeros((V * H * W, n * n * n))
-    for k in range(n * n * n):
-        e = torch.zeros(n * n * n, device="cuda")
-        e[k] = 1.0
-        A[:, k] = ops.forward_project(e.view(n, n, n), ang, h, det, grid).cpu().numpy().ravel()
-    At = np.zeros((n * n * n, V * H * W))
-    for k in range(V * H * W):
-        e = torch.zeros(V * H * W, device="cuda")
-        e[k] = 1.0
-        At[:, k] = ops.backproject(e.view(V, H, W), ang, h, det, grid).cpu().numpy().ravel()
+def test_forward_is_the_exact_transpose(tmp_path, vs, uoff, heights):
+    """Every matrix element: A e_voxel (forward projector) against A^T e_pixel, with the
+    backprojector forced to the global-gather kernel and to the shared-memory one (its pair loop
+    and per-voxel loops): all form rows the same way and take the same decisions."""
+    A, At = transpose_matrices(tmp_path, "global", vs, uoff, heights)
     assert np.count_nonzero(A) > 100
     assert np.array_equal(A != 0, At.T != 0)
     np.testing.assert_allclose(A, At.T, rtol=1e-6, atol=1e-7)
+    A2, At2 = transpose_matrices(tmp_path, "tma", vs, uoff, heights)
+    assert np.array_equal(A2, A)
+    assert np.array_equal(A != 0, At2.T != 0)
+    np.testing.assert_allclose(A, At2.T, rtol=1e-6, atol=1e-7)
 
 
 def test_emit_signals_off_silences_callbacks(tmp_path):

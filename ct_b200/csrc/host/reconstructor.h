@@ -42,7 +42,9 @@ struct HostBuf {
 // active device). Buffers only grow and are reused across reconstructions.
 struct DeviceWork {
     int device = 0;
-    cudaStream_t s_copy = nullptr, s_comp = nullptr, s_down = nullptr;
+    // uploads, backprojection (and layout), downloads; filtering on s_filt at the
+    // greatest stream priority, beside the early slabs' backprojection
+    cudaStream_t s_copy = nullptr, s_comp = nullptr, s_down = nullptr, s_filt = nullptr;
     DevBuf d_filtered, d_ring, d_views, d_angles, d_heights, d_tw, d_K, d_slab[3], d_conv[3];
     HostBuf h_stage[2];
     int tables_key[3] = {-1, -1, -1};  // W, pad, filter of the cached tables
